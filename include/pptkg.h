@@ -1,0 +1,168 @@
+/*
+ * pptkg.h -- C ABI of pptk_b200, the B200 implementation of pptk's k-d tree,
+ * kNN / r-near queries and PCA normal estimation.
+ *
+ * Plain pointers and sizes only.  Every function returns PPTKG_OK (0) or a
+ * PPTKG_E_* status; pptkg_last_error() returns the message of the last
+ * failure on the calling thread.  Array arguments are host memory when
+ * `mem` is PPTKG_MEM_HOST and device memory of the current device when it is
+ * PPTKG_MEM_DEVICE; `stream` is a cudaStream_t (NULL: the default stream).
+ * Calls return once their results are written.
+ *
+ * The reference interfaces that each entry point replaces are cited with
+ * paths relative to the pptk source tree.
+ */
+#ifndef PPTKG_H_
+#define PPTKG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PPTKG_API __attribute__((visibility("default")))
+#else
+#define PPTKG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PPTKG_OK 0
+#define PPTKG_E_INVALID 1     /* bad argument value (Python: ValueError) */
+#define PPTKG_E_TYPE 2        /* unsupported dtype or dim (TypeError) */
+#define PPTKG_E_CUDA 3        /* CUDA runtime failure */
+#define PPTKG_E_RANGE 4       /* index outside the point range (RuntimeError) */
+#define PPTKG_E_DEVICE 5      /* a kernel's internal check failed */
+#define PPTKG_E_UNSUPPORTED 6 /* not implemented (NotImplementedError) */
+
+/* element types (numpy dtypes of the reference's dispatch,
+ * pptk/kdtree/kdtree_wrapper.cpp:15-41) */
+#define PPTKG_F32 0
+#define PPTKG_F64 1
+#define PPTKG_I8 2
+#define PPTKG_I16 3
+#define PPTKG_I32 4
+#define PPTKG_I64 5
+#define PPTKG_U8 6
+#define PPTKG_U16 7
+#define PPTKG_U32 8
+#define PPTKG_U64 9
+
+#define PPTKG_MEM_HOST 0
+#define PPTKG_MEM_DEVICE 1
+
+/* normal-estimation arithmetic */
+#define PPTKG_PREC_AUTO 0 /* float32 input: FP32 path; float64 input: FP64 */
+#define PPTKG_PREC_FP32 1 /* FP32 covariance (shifted, compensated) + FP32
+                             eigensolve, FP64 re-solve of small eigen-gaps */
+#define PPTKG_PREC_FP64 2
+
+typedef struct pptkg_tree pptkg_tree;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+PPTKG_API int pptkg_version(void);
+
+/* Copies the last error message of this thread into buf (NUL-terminated,
+ * truncated to len); returns the status of that error. */
+PPTKG_API int pptkg_last_error(char* buf, size_t len);
+
+/* Builds a k-d tree over n points of `dim` coordinates (contiguous rows).
+ * Replaces pptk.kdtree._build: Build + BuildTreeAction
+ * (pptk/kdtree/kdtree_wrapper.cpp:76-104, :281-304) and the KdTree
+ * constructor (pptk/kdtree/src/kdtree-impl.h:773-833).  Rows holding a NaN or
+ * inf coordinate are left out, as in the reference.  The tree owns a copy of
+ * the points.  dtype: PPTKG_F32 or PPTKG_F64; dim: 2, 3 or 4. */
+PPTKG_API int pptkg_tree_build(const void* points, int64_t n, int dim, int dtype, int mem, int max_leaf_size,
+                     double empty_split, void* stream, pptkg_tree** out);
+
+/* Frees a tree.  Replaces DeleteKdTree (kdtree_wrapper.cpp:57-74). */
+PPTKG_API int pptkg_tree_free(pptkg_tree* tree);
+
+/* Sizes of a tree: input rows, valid rows (the reference's num_points(),
+ * kdtree.h:224), dim, dtype, build records, traversal depth bound. */
+PPTKG_API int pptkg_tree_info(const pptkg_tree* tree, int64_t* n, int64_t* n_valid, int* dim, int* dtype,
+                    int64_t* n_records, int* depth);
+
+/* Tree position -> original row (n_valid entries): the reference's
+ * reverse_indices() (kdtree.h:226). */
+PPTKG_API int pptkg_tree_reverse_indices(const pptkg_tree* tree, int32_t* out, int mem, void* stream);
+
+/* The reference node list in preorder, 5 doubles per node (split dim, split
+ * index, split value, has left child, has right child), empty-split nodes
+ * included (pptk/kdtree/src/node.h:15-29).  *count receives the node count;
+ * out may be NULL to query it. */
+PPTKG_API int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, int64_t* count);
+
+/* Re-cuts the traversal hierarchy at `bucket` points per leaf bucket (a
+ * tuning knob; results do not depend on it). */
+PPTKG_API int pptkg_tree_set_bucket(pptkg_tree* tree, int bucket, void* stream);
+
+/* k nearest neighbours of m point queries (rows of `dim` coordinates of
+ * qdtype F32/F64) with distance < dmax.  out_idx: m x k original row indices
+ * in ascending distance (ties: ascending tree position), -1 padded; out_cnt
+ * (optional): neighbours found.  Replaces QueryWithPoints with k > 0
+ * (kdtree_wrapper.cpp:139-159) / KdTree::KNearestNeighbors
+ * (kdtree-impl.h:873-929).  1 <= k <= 64. */
+PPTKG_API int pptkg_knn(const pptkg_tree* tree, const void* queries, int64_t m, int qdtype, int mem, int k, double dmax,
+              int32_t* out_idx, int32_t* out_cnt, void* stream);
+
+/* k nearest neighbours of stored points given by original row index
+ * (indices NULL: rows 0..m-1), each point excluding itself.  Replaces
+ * QueryWithIndices with k > 0 (kdtree_wrapper.cpp:117-137) /
+ * KNearestNeighborsSelf (kdtree-impl.h:931-976).  A row dropped at build
+ * time gets no neighbours. */
+PPTKG_API int pptkg_knn_self(const pptkg_tree* tree, const int32_t* indices, int64_t m, int mem, int k, double dmax,
+                   int32_t* out_idx, int32_t* out_cnt, void* stream);
+
+/* r-near, first step: per-query counts of points with distance < dmax,
+ * written as offsets (m + 1 entries, out_offsets[m] = total).  Queries are
+ * points (queries != NULL) or stored rows (indices, or rows 0..m-1 when both
+ * are NULL; the row itself excluded).  Replaces the counting half of
+ * RNearNeighbors[Self] (kdtree-impl.h:978-1069). */
+PPTKG_API int pptkg_rnear_count(const pptkg_tree* tree, const void* queries, const int32_t* indices, int64_t m, int qdtype,
+                      int mem, double dmax, int64_t* out_offsets, int64_t* total, void* stream);
+
+/* r-near, second step: the hits of each query in ascending tree position
+ * (the reference's left-then-right order, kdtree-impl.h:519-558), as original
+ * row indices at out_idx[offsets[i] .. offsets[i+1]). */
+PPTKG_API int pptkg_rnear_fill(const pptkg_tree* tree, const void* queries, const int32_t* indices, int64_t m, int qdtype,
+                     int mem, double dmax, const int64_t* offsets, int32_t* out_idx, void* stream);
+
+/* PCA normals: builds a tree over n x 3 points and, for every point (or the
+ * m rows in `subsample`), eigen-decomposes the covariance of its k nearest
+ * neighbours including itself within distance r (k = -1: all points within
+ * r).  Replaces estimate_normals (pptk/processing/estimate_normals/
+ * estimate_normals.cpp:17-120, :259-345).  num_eigen 1: out_evecs m x 3 (the
+ * normal), out_evals m; num_eigen 3: m x 3 x 3 ([i, j, :] = j-th eigenvector,
+ * ascending eigenvalue) and m x 3.  Outputs may be NULL. */
+PPTKG_API int pptkg_estimate_normals(const void* points, int64_t n, int dtype, int mem, int k, float r,
+                           const int32_t* subsample, int64_t m, int num_eigen, int precision, void* out_evecs,
+                           void* out_evals, int32_t* out_sizes, void* stream);
+
+/* The same PCA over an existing 3-D tree (rows of the tree's input). */
+PPTKG_API int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices, int64_t m, int mem, int k, float r,
+                       int num_eigen, int precision, void* out_evecs, void* out_evals, int32_t* out_sizes,
+                       void* stream);
+
+/* Batched symmetric 3x3 eigensolve of m row-major matrices of dtype F32/F64:
+ * w m x 3 ascending; V m x 3 x 3 with layout 0: V[i, :, j] = j-th
+ * eigenvector (vfuncs._eigh, pptk/vfuncs/vfuncs.cpp:1241-1293), layout 1:
+ * V[i, j, :] = j-th eigenvector (estimate_normals.cpp:96-99). */
+PPTKG_API int pptkg_eigh3(const void* A, int64_t m, int dtype, int mem, void* w, void* V, int layout, void* stream);
+
+/* Instrumentation (no reference counterpart).  Stage timing records CUDA
+ * events on the launching stream around each stage ("build", "order",
+ * "knn", "normals", "rnear_count", "rnear_fill", "h2d", "d2h");
+ * enabling or disabling resets the totals. */
+PPTKG_API int pptkg_profile_enable(int on);
+PPTKG_API int pptkg_profile_get(const char* stage, double* total_ms, int64_t* count);
+/* Kernels launched by this library since it was loaded. */
+PPTKG_API int64_t pptkg_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PPTKG_H_ */

@@ -1,0 +1,1026 @@
+// Level-synchronous device builder that reproduces the reference k-d tree
+// exactly (pptk/kdtree/src/kdtree-impl.h:248-329 MakeNode /
+// RecursiveBuildHelper, :773-818 BuildTree).
+//
+// The reference builds depth first; every node only permutes the indices of
+// its own range, so building all nodes of a level at once gives the same
+// permutation.  Nodes with more than `small_cap` points are processed by
+// grid-wide kernels over 4096-point tiles; smaller subtrees are finished by
+// one CTA each, entirely in shared memory.
+//
+// The reference partition (PartitionIndices, kdtree-impl.h:192-246) is two
+// Hoare passes with converging cursors.  Each pass pairs the j-th misplaced
+// element of the left zone (ascending) with the j-th misplaced element of the
+// right zone (descending), so it is reproduced by ranking the two kinds of
+// misplaced elements with scans and swapping rank-matched pairs.
+#include <algorithm>
+#include <vector>
+
+#include "build.cuh"
+#include "profile.cuh"
+#include "util.cuh"
+
+namespace pptkg {
+
+constexpr int BT = 256;     // threads per tile block
+constexpr int TILE = 4096;  // points per tile
+constexpr int TITEMS = TILE / BT;
+
+template <typename T, int D>
+struct Seg {
+  int b, e;
+  int parent, side;
+  int lvl;
+  int rec;
+  T lo[D], hi[D];  // loose extent (the reference's node_box), trimmed in place
+  typename OrdOf<T>::type tlo[D], thi[D];
+  int act;
+  int sd;
+  T sv;
+  int L1, L2;
+  int G;
+  int tile0, ntiles;
+};
+
+struct BuildCtl {
+  int n_tiles;
+  int nB;
+  int nSmall;
+  int rec_count;
+  int depth;
+  int status;
+};
+
+// ----------------------------------------------------------------- helpers
+template <typename T>
+__device__ __forceinline__ T midpoint_ref(T a, T b) {
+  // kdtree-impl.h:167-173 (signed / floating form)
+  if ((a >= (T)0 && b >= (T)0) || (a < (T)0 && b < (T)0)) return xadd(xdiv(xsub(b, a), (T)2), a);
+  return xdiv(xadd(a, b), (T)2);
+}
+
+__device__ __forceinline__ double max0(double x) { return (0.0 < x) ? x : 0.0; }
+
+// MakeNode's per-node decisions (kdtree-impl.h:248-297): empty-space trims of
+// the loose extent against the tight box (TrimEmptyGaps, :114-158, in double),
+// then the leaf test and the widest-axis midpoint split (ComputeSplit,
+// :175-190, in T).  Writes the record except split_index and children.
+template <typename T, int D>
+__device__ void node_logic(int size, long long n_orig, bool is_top, T lo[D], T hi[D], const T tlo[D], const T thi[D],
+                           int max_leaf, double thr, Rec<T, D>& rec, int& act, int& sd, T& sv) {
+  for (int i = 0; i < D; i++) {
+    rec.lo[i] = tlo[i];
+    rec.hi[i] = thi[i];
+  }
+  if (is_top)
+    for (int i = 0; i < D; i++) {
+      lo[i] = tlo[i];
+      hi[i] = thi[i];
+    }
+  rec.ntrim = 0;
+  rec.split_dim = -1;
+  rec.split_val = (T)0;
+  rec.split_index = -1;
+  rec.left = rec.right = -1;
+  if ((long long)size != n_orig) {
+    for (int guard = 0; guard <= 2 * D; guard++) {
+      int gdim = -1, gside = -1;
+      double gsize = 0.0;
+      for (int i = 0; i < D; i++) {
+        double g = max0(__dsub_rn((double)hi[i], (double)thi[i]));
+        if (g >= gsize) gdim = i, gside = 1, gsize = g;
+        g = max0(__dsub_rn((double)tlo[i], (double)lo[i]));
+        if (g >= gsize) gdim = i, gside = 0, gsize = g;
+      }
+      if (gsize == 0.0) break;
+      double width = __dsub_rn((double)hi[gdim], (double)lo[gdim]);
+      if (__ddiv_rn(gsize, width) <= thr) break;
+      if (rec.ntrim < 2 * D) rec.trim[rec.ntrim] = (uint8_t)(gdim * 2 + gside);
+      rec.ntrim++;
+      if (gside == 0)
+        lo[gdim] = tlo[gdim];
+      else
+        hi[gdim] = thi[gdim];
+    }
+  }
+  bool point = true;
+  for (int i = 0; i < D; i++)
+    if (tlo[i] != thi[i]) point = false;
+  act = 0;
+  if (!point && size > max_leaf) {
+    T maxw = (T)0;
+    sd = 0;
+    sv = (T)0;
+    for (int i = 0; i < D; i++) {
+      T w = xsub(thi[i], tlo[i]);
+      if (w >= maxw) {
+        maxw = w;
+        sd = i;
+        sv = (tlo[i] == thi[i]) ? tlo[i] : midpoint_ref(tlo[i], thi[i]);
+      }
+    }
+    act = 1;
+    rec.split_dim = (int8_t)sd;
+    rec.split_val = sv;
+  }
+}
+
+// num_left rule of PartitionIndices (kdtree-impl.h:234-244).
+__device__ __forceinline__ int num_left_rule(int lim1, int lim2, int count) {
+  int nl;
+  if (lim1 > count / 2)
+    nl = lim1;
+  else if (lim2 < count / 2)
+    nl = lim2;
+  else
+    nl = count / 2;
+  if (lim1 == count && lim2 == 0) nl = count / 2;
+  return nl;
+}
+
+// ------------------------------------------------------- input staging ----
+template <typename T, int D>
+__global__ void k_valid(const T* __restrict__ in, int64_t n, int* __restrict__ flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < D; d++) ok = ok && isfinite(in[i * D + d]);
+  flag[i] = ok ? 1 : 0;
+}
+
+template <typename T, int D>
+__global__ void k_compact(const T* __restrict__ in, int64_t n, const int* __restrict__ flag,
+                          const int* __restrict__ off, SoA<T, D> soa) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !flag[i]) return;
+  int j = off[i];
+#pragma unroll
+  for (int d = 0; d < D; d++) soa.x[d][j] = in[i * D + d];
+  soa.id[j] = (int)i;
+}
+
+// ------------------------------------------------------ grid-wide levels --
+template <typename T, int D>
+__global__ void k_tiles(Seg<T, D>* segs, int nseg, int* tile_seg, BuildCtl* ctl) {
+  __shared__ int sh[33];
+  int carry = 0;
+  for (int c0 = 0; c0 < nseg; c0 += blockDim.x) {
+    int i = c0 + threadIdx.x;
+    int nt = 0;
+    if (i < nseg) nt = div_up_dev(segs[i].e - segs[i].b, TILE);
+    int tot;
+    int ex = block_excl_scan(nt, sh, tot);
+    if (i < nseg) {
+      segs[i].tile0 = carry + ex;
+      segs[i].ntiles = nt;
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0) ctl->n_tiles = carry;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = wid; i < nseg; i += nw) {
+    int t0 = segs[i].tile0, nt = segs[i].ntiles;
+    for (int t = lane; t < nt; t += 32) tile_seg[t0 + t] = i;
+  }
+}
+
+template <typename T, int D>
+__device__ __forceinline__ bool tile_range(const Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, int& s,
+                                           int& start, int& end) {
+  int t = blockIdx.x;
+  if (t >= ctl->n_tiles) return false;
+  s = tile_seg[t];
+  start = segs[s].b + (t - segs[s].tile0) * TILE;
+  end = min(start + TILE, segs[s].e);
+  return true;
+}
+
+template <typename T, int D>
+__global__ void k_seg_init(Seg<T, D>* segs, int nseg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg) return;
+  for (int d = 0; d < D; d++) {
+    segs[i].tlo[d] = ord_of(Limits<T>::max());
+    segs[i].thi[d] = ord_of(Limits<T>::lowest());
+  }
+  segs[i].L1 = segs[i].L2 = 0;
+  segs[i].act = 0;
+  segs[i].G = 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(BT) k_bbox(Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, SoA<T, D> soa) {
+  int s, start, end;
+  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
+  __shared__ T shmn[D][BT / 32], shmx[D][BT / 32];
+  T mn[D], mx[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    mn[d] = Limits<T>::max();
+    mx[d] = Limits<T>::lowest();
+  }
+  for (int i = start + threadIdx.x; i < end; i += BT) {
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      T v = soa.x[d][i];
+      mn[d] = min(mn[d], v);
+      mx[d] = max(mx[d], v);
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    mn[d] = warp_min(mn[d]);
+    mx[d] = warp_max(mx[d]);
+    if (lane == 0) {
+      shmn[d][wid] = mn[d];
+      shmx[d][wid] = mx[d];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < D) {
+    int d = threadIdx.x;
+    T a = shmn[d][0], b = shmx[d][0];
+    for (int w = 1; w < BT / 32; w++) {
+      a = min(a, shmn[d][w]);
+      b = max(b, shmx[d][w]);
+    }
+    atomicMin(&segs[s].tlo[d], ord_of(a));
+    atomicMax(&segs[s].thi[d], ord_of(b));
+  }
+}
+
+template <typename T, int D>
+__global__ void k_node(Seg<T, D>* segs, int nseg, int rec_base, Rec<T, D>* recs, long long n_orig, int max_leaf,
+                       double thr) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg) return;
+  Seg<T, D>& g = segs[i];
+  T tlo[D], thi[D], lo[D], hi[D];
+  for (int d = 0; d < D; d++) {
+    tlo[d] = from_ord(g.tlo[d]);
+    thi[d] = from_ord(g.thi[d]);
+    lo[d] = g.lo[d];
+    hi[d] = g.hi[d];
+  }
+  Rec<T, D> rec;
+  int act, sd = 0;
+  T sv = (T)0;
+  node_logic<T, D>(g.e - g.b, n_orig, g.parent < 0, lo, hi, tlo, thi, max_leaf, thr, rec, act, sd, sv);
+  rec.begin = g.b;
+  rec.end = g.e;
+  const int id = rec_base + i;
+  recs[id] = rec;
+  if (g.parent >= 0) {
+    if (g.side == 0)
+      recs[g.parent].left = id;
+    else
+      recs[g.parent].right = id;
+  }
+  g.rec = id;
+  g.act = act;
+  g.sd = sd;
+  g.sv = sv;
+  for (int d = 0; d < D; d++) {
+    g.lo[d] = lo[d];
+    g.hi[d] = hi[d];
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(BT) k_count(Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, SoA<T, D> soa) {
+  int s, start, end;
+  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
+  if (!segs[s].act) return;
+  __shared__ long long sh[33];
+  const T sv = segs[s].sv;
+  const T* v = soa.x[segs[s].sd];
+  int c1 = 0, c2 = 0;
+  for (int i = start + threadIdx.x; i < end; i += BT) {
+    T x = v[i];
+    c1 += x < sv;
+    c2 += x <= sv;
+  }
+  long long packed = ((long long)c2 << 32) | (long long)c1;
+  long long tot = block_sum(packed, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(&segs[s].L1, (int)(tot & 0xffffffffll));
+    atomicAdd(&segs[s].L2, (int)(tot >> 32));
+  }
+}
+
+// Misplaced-element predicates of the two partition passes.
+template <typename T>
+__device__ __forceinline__ void pass_flags(int pass, int i, T x, T sv, int b, int L1, int L2, bool& bl, bool& gr) {
+  if (pass == 1) {
+    const int Z = b + L1;
+    bl = (i < Z) && !(x < sv);
+    gr = (i >= Z) && (x < sv);
+  } else {
+    const int Z = b + L2;
+    bl = (i >= b + L1) && (i < Z) && (x > sv);
+    gr = (i >= Z) && (x <= sv);
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(BT) k_flags(int pass, Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl,
+                                              SoA<T, D> soa, long long* tile_cnt) {
+  int s, start, end;
+  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
+  __shared__ long long sh[33];
+  long long c = 0;
+  if (segs[s].act) {
+    const T sv = segs[s].sv;
+    const T* v = soa.x[segs[s].sd];
+    const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2;
+    for (int i = start + threadIdx.x; i < end; i += BT) {
+      bool bl, gr;
+      pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
+      c += (long long)bl + ((long long)gr << 32);
+    }
+  }
+  long long tot = block_sum(c, sh);
+  if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
+}
+
+template <typename T, int D>
+__global__ void k_tscan(Seg<T, D>* segs, const long long* tile_cnt, long long* tile_off, BuildCtl* ctl) {
+  __shared__ long long sh[33];
+  Seg<T, D>& g = segs[blockIdx.x];
+  if (!g.act) return;
+  long long carry = 0;
+  for (int c0 = 0; c0 < g.ntiles; c0 += blockDim.x) {
+    int t = c0 + threadIdx.x;
+    long long v = t < g.ntiles ? tile_cnt[g.tile0 + t] : 0;
+    long long tot;
+    long long ex = block_excl_scan(v, sh, tot);
+    if (t < g.ntiles) tile_off[g.tile0 + t] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) {
+    int nbl = (int)(carry & 0xffffffffll), ngr = (int)(carry >> 32);
+    g.G = nbl;
+    if (nbl != ngr) atomicExch(&ctl->status, 1);
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(BT) k_scatter(int pass, Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl,
+                                                SoA<T, D> soa, const long long* tile_off, int* blpos, int* grpos) {
+  int s, start, end;
+  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
+  if (!segs[s].act) return;
+  __shared__ long long sh[33];
+  const T sv = segs[s].sv;
+  const T* v = soa.x[segs[s].sd];
+  const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2, G = segs[s].G;
+  const int i0 = start + threadIdx.x * TITEMS;
+  unsigned mbl = 0, mgr = 0;
+#pragma unroll
+  for (int j = 0; j < TITEMS; j++) {
+    int i = i0 + j;
+    if (i < end) {
+      bool bl, gr;
+      pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
+      mbl |= (unsigned)bl << j;
+      mgr |= (unsigned)gr << j;
+    }
+  }
+  long long mine = (long long)__popc(mbl) + ((long long)__popc(mgr) << 32);
+  long long tot;
+  long long ex = block_excl_scan(mine, sh, tot) + tile_off[blockIdx.x];
+  int rb = (int)(ex & 0xffffffffll), rg = (int)(ex >> 32);
+  const int size = segs[s].e - b;
+#pragma unroll
+  for (int j = 0; j < TITEMS; j++) {
+    if (mbl >> j & 1) {
+      if (rb < size) blpos[b + rb] = i0 + j;
+      rb++;
+    }
+    if (mgr >> j & 1) {
+      const int slot = G - 1 - rg;
+      if (slot >= 0 && slot < size) grpos[b + slot] = i0 + j;
+      rg++;
+    }
+  }
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(BT) k_swap(Seg<T, D>* segs, const int* tile_seg, BuildCtl* ctl, SoA<T, D> soa,
+                                             const int* blpos, const int* grpos) {
+  int s, start, end;
+  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
+  if (!segs[s].act) return;
+  const int b = segs[s].b, e = segs[s].e, G = segs[s].G;
+  for (int i = start + threadIdx.x; i < end; i += BT) {
+    int j = i - b;
+    if (j >= G) break;
+    int x = blpos[b + j], y = grpos[b + j];
+    if (x < b || x >= e || y < b || y >= e) {
+      atomicExch(&ctl->status, 4);
+      continue;
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      T t = soa.x[d][x];
+      soa.x[d][x] = soa.x[d][y];
+      soa.x[d][y] = t;
+    }
+    int t = soa.id[x];
+    soa.id[x] = soa.id[y];
+    soa.id[y] = t;
+  }
+}
+
+template <typename T, int D>
+__global__ void k_children(Seg<T, D>* segs, int nseg, Rec<T, D>* recs, Seg<T, D>* next, Seg<T, D>* small,
+                           int small_cap_pts, BuildCtl* ctl) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg) return;
+  const Seg<T, D>& g = segs[i];
+  if (!g.act) return;
+  const int count = g.e - g.b;
+  const int si = g.b + num_left_rule(g.L1, g.L2, count);
+  recs[g.rec].split_index = si;
+  for (int side = 0; side < 2; side++) {
+    int cb = side ? si : g.b, ce = side ? g.e : si;
+    if (cb >= ce) continue;
+    Seg<T, D> c;
+    c.b = cb;
+    c.e = ce;
+    c.parent = g.rec;
+    c.side = side;
+    c.lvl = g.lvl + 1;
+    for (int d = 0; d < D; d++) {
+      c.lo[d] = g.lo[d];
+      c.hi[d] = g.hi[d];
+    }
+    if (side == 0)
+      c.hi[g.sd] = g.sv;
+    else
+      c.lo[g.sd] = g.sv;
+    if (ce - cb > small_cap_pts)
+      next[atomicAdd(&ctl->nB, 1)] = c;
+    else
+      small[atomicAdd(&ctl->nSmall, 1)] = c;
+  }
+}
+
+// -------------------------------------------------- per-CTA subtrees ----
+template <typename T, int D>
+struct Entry {
+  int b, e, parent, side;
+  T lo[D], hi[D];
+};
+
+constexpr int SUB_THREADS = 256;
+
+// Finishes one small segment's whole subtree in shared memory, one warp per
+// node, level by level.
+template <typename T, int D>
+__global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small, SoA<T, D> soa, Rec<T, D>* recs,
+                                                         int cap_pts, int cap_list, long long n_orig, int max_leaf,
+                                                         double thr, int rec_cap, BuildCtl* ctl) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Seg<T, D> seg = small[blockIdx.x];
+  const int n = seg.e - seg.b;
+  T* X[D];
+  unsigned char* p = smem;
+  for (int d = 0; d < D; d++) {
+    X[d] = (T*)p;
+    p += sizeof(T) * cap_pts;
+  }
+  int* ID = (int*)p;
+  p += sizeof(int) * cap_pts;
+  int* S = (int*)p;
+  p += sizeof(int) * cap_pts;
+  p = (unsigned char*)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+  Entry<T, D>* LA = (Entry<T, D>*)p;
+  Entry<T, D>* LB = LA + cap_list;
+  int* cnt = (int*)(LB + cap_list);  // [0] nA, [1] nB, [2] base, [3] overflow
+
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int d = 0; d < D; d++) X[d][i] = soa.x[d][seg.b + i];
+    ID[i] = soa.id[seg.b + i];
+  }
+  if (threadIdx.x == 0) {
+    Entry<T, D> r;
+    r.b = 0;
+    r.e = n;
+    r.parent = seg.parent;
+    r.side = seg.side;
+    for (int d = 0; d < D; d++) {
+      r.lo[d] = seg.lo[d];
+      r.hi[d] = seg.hi[d];
+    }
+    LA[0] = r;
+    cnt[0] = 1;
+    cnt[3] = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int levels = 0;
+  while (true) {
+    const int nA = cnt[0];
+    if (nA == 0) break;
+    if (levels > n + 1) {  // every level splits ranges into strictly smaller ones
+      if (threadIdx.x == 0) atomicExch(&ctl->status, 5);
+      break;
+    }
+    if (threadIdx.x == 0) {
+      cnt[1] = 0;
+      cnt[2] = atomicAdd(&ctl->rec_count, nA);
+    }
+    __syncthreads();
+    const int base = cnt[2];
+    levels++;
+    for (int ei = wid; ei < nA; ei += nw) {
+      Entry<T, D> en = LA[ei];
+      const int b = en.b, e = en.e, size = e - b;
+      T mn[D], mx[D];
+      for (int d = 0; d < D; d++) {
+        mn[d] = Limits<T>::max();
+        mx[d] = Limits<T>::lowest();
+      }
+      for (int q = b + lane; q < e; q += 32)
+        for (int d = 0; d < D; d++) {
+          T v = X[d][q];
+          mn[d] = min(mn[d], v);
+          mx[d] = max(mx[d], v);
+        }
+      for (int d = 0; d < D; d++) {
+        mn[d] = warp_min(mn[d]);
+        mx[d] = warp_max(mx[d]);
+      }
+      int act = 0, sd = 0;
+      T sv = (T)0;
+      const int id = base + ei;
+      if (lane == 0) {
+        Rec<T, D> rec;
+        node_logic<T, D>(size, n_orig, en.parent < 0, en.lo, en.hi, mn, mx, max_leaf, thr, rec, act, sd, sv);
+        rec.begin = seg.b + b;
+        rec.end = seg.b + e;
+        if (id >= rec_cap) {
+          atomicExch(&ctl->status, 6);
+          act = 0;
+        } else {
+          recs[id] = rec;
+        }
+        if (en.parent >= 0 && id < rec_cap) {
+          if (en.side == 0)
+            recs[en.parent].left = id;
+          else
+            recs[en.parent].right = id;
+        }
+        LA[ei] = en;  // keep the trimmed extent for the children
+      }
+      act = __shfl_sync(0xffffffffu, act, 0);
+      if (!act) continue;
+      sd = __shfl_sync(0xffffffffu, sd, 0);
+      sv = __shfl_sync(0xffffffffu, sv, 0);
+      T* v = X[sd];
+      int L1 = 0, L2 = 0;
+      for (int q0 = b; q0 < e; q0 += 32) {
+        int q = q0 + lane;
+        T x = q < e ? v[q] : sv;
+        bool in = q < e;
+        L1 += __popc(__ballot_sync(0xffffffffu, in && x < sv));
+        L2 += __popc(__ballot_sync(0xffffffffu, in && x <= sv));
+      }
+      const int half = size / 2;
+      for (int pass = 1; pass <= 2; pass++) {
+        const int zlo = pass == 1 ? b : b + L1;
+        const int Z = pass == 1 ? b + L1 : b + L2;
+        int G = 0;
+        for (int q0 = zlo; q0 < Z; q0 += 32) {
+          int q = q0 + lane;
+          bool f = false;
+          if (q < Z) {
+            T x = v[q];
+            f = pass == 1 ? !(x < sv) : (x > sv);
+          }
+          unsigned bal = __ballot_sync(0xffffffffu, f);
+          if (f) S[b + G + __popc(bal & lt)] = q;
+          G += __popc(bal);
+        }
+        int a = 0;
+        for (int q0 = Z; q0 < e; q0 += 32) {
+          int q = q0 + lane;
+          bool f = false;
+          if (q < e) {
+            T x = v[q];
+            f = pass == 1 ? (x < sv) : (x <= sv);
+          }
+          unsigned bal = __ballot_sync(0xffffffffu, f);
+          if (f) {
+            int r = a + __popc(bal & lt);
+            if (r < G) S[b + half + (G - 1 - r)] = q;
+          }
+          a += __popc(bal);
+        }
+        if (a != G && lane == 0) atomicExch(&ctl->status, 2);
+        __syncwarp();
+        for (int j = lane; j < G; j += 32) {
+          int x = S[b + j], y = S[b + half + j];
+          for (int d = 0; d < D; d++) {
+            T t = X[d][x];
+            X[d][x] = X[d][y];
+            X[d][y] = t;
+          }
+          int t = ID[x];
+          ID[x] = ID[y];
+          ID[y] = t;
+        }
+        __syncwarp();
+      }
+      if (lane == 0) {
+        const int si = b + num_left_rule(L1, L2, size);
+        if (id < rec_cap) recs[id].split_index = seg.b + si;
+        const Entry<T, D> par = LA[ei];
+        for (int side = 0; side < 2; side++) {
+          int cb = side ? si : b, ce = side ? e : si;
+          if (cb >= ce) continue;
+          Entry<T, D> c;
+          c.b = cb;
+          c.e = ce;
+          c.parent = id;
+          c.side = side;
+          for (int d = 0; d < D; d++) {
+            c.lo[d] = par.lo[d];
+            c.hi[d] = par.hi[d];
+          }
+          if (side == 0)
+            c.hi[sd] = sv;
+          else
+            c.lo[sd] = sv;
+          int slot = atomicAdd(&cnt[1], 1);
+          if (slot < cap_list)
+            LB[slot] = c;
+          else
+            atomicExch(&cnt[3], 1);
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      cnt[0] = min(cnt[1], cap_list);
+      if (cnt[3]) atomicExch(&ctl->status, 3);
+    }
+    __syncthreads();
+    Entry<T, D>* tmp = LA;
+    LA = LB;
+    LB = tmp;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int d = 0; d < D; d++) soa.x[d][seg.b + i] = X[d][i];
+    soa.id[seg.b + i] = ID[i];
+  }
+  if (threadIdx.x == 0) atomicMax(&ctl->depth, seg.lvl + levels);
+}
+
+// ------------------------------------------------------- finishing ----
+template <typename T, int D>
+__global__ void k_finish(SoA<T, D> soa, int nv, PointRec<T, D>* pts, int* fwd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  PointRec<T, D> r;
+#pragma unroll
+  for (int d = 0; d < D; d++) r.c[d] = soa.x[d][i];
+  r.id = soa.id[i];
+  pts[i] = r;
+  fwd[r.id] = i;
+}
+
+template <typename T, int D>
+__global__ void k_tflag(const Rec<T, D>* recs, int n_recs, int bucket, int* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_recs) return;
+  const Rec<T, D>& r = recs[i];
+  flag[i] = (r.split_dim >= 0 && r.end - r.begin > bucket && r.left >= 0 && r.right >= 0) ? 1 : 0;
+}
+
+template <typename T, int D>
+__global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, const int* tid, TNode<T, D>* nodes) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_recs || !flag[i]) return;
+  const Rec<T, D>& r = recs[i];
+  TNode<T, D> t;
+  for (int c = 0; c < 2; c++) {
+    int ch = c ? r.right : r.left;
+    const Rec<T, D>& cr = recs[ch];
+    for (int d = 0; d < D; d++) {
+      t.lo[c][d] = cr.lo[d];
+      t.hi[c][d] = cr.hi[d];
+    }
+    t.cnt[c] = cr.end - cr.begin;
+    t.ref[c] = flag[ch] ? tid[ch] : -cr.begin - 1;
+  }
+  nodes[tid[i]] = t;
+}
+
+// Root-is-a-bucket tree (or empty tree): a single node whose first child is
+// the whole point range.
+template <typename T, int D>
+__global__ void k_tsingle(const Rec<T, D>* recs, int n_recs, int nv, TNode<T, D>* nodes) {
+  TNode<T, D> t;
+  for (int c = 0; c < 2; c++)
+    for (int d = 0; d < D; d++) {
+      t.lo[c][d] = Limits<T>::max();
+      t.hi[c][d] = Limits<T>::lowest();
+    }
+  t.ref[0] = -1;
+  t.ref[1] = -1;
+  t.cnt[0] = 0;
+  t.cnt[1] = 0;
+  if (n_recs > 0 && nv > 0) {
+    for (int d = 0; d < D; d++) {
+      t.lo[0][d] = recs[0].lo[d];
+      t.hi[0][d] = recs[0].hi[d];
+    }
+    t.cnt[0] = nv;
+  }
+  nodes[0] = t;
+}
+
+// ------------------------------------------------------------ host side ----
+template <typename T, int D>
+int small_capacity(int max_leaf, int& cap_list, size_t& smem) {
+  const size_t budget = 160 * 1024;
+  int cap = sizeof(T) == 4 ? 4096 : 2048;
+  while (true) {
+    cap_list = 2 * (cap / (max_leaf + 1)) + 2;
+    smem = (sizeof(T) * D + 2 * sizeof(int)) * (size_t)cap + 16 + 2 * sizeof(Entry<T, D>) * (size_t)cap_list +
+           4 * sizeof(int);
+    if (smem <= budget || cap <= 64) break;
+    cap /= 2;
+  }
+  return cap;
+}
+
+template <typename T, int D>
+TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int bucket, cudaStream_t st) {
+  if (n > (int64_t)INT32_MAX - 1) throw Error(E_INVALID, "k-d tree supports at most 2^31-2 points");
+  if (max_leaf < 1) max_leaf = 1;
+  Stage stage("build", st);
+  std::unique_ptr<TreeBase> tree(new TreeBase());
+  tree->dtype = sizeof(T) == 4 ? F32 : F64;
+  tree->dim = D;
+  tree->n = n;
+  tree->max_leaf = max_leaf;
+  tree->empty_split = thr;
+  tree->bucket = bucket;
+  PPTKG_CUDA(cudaGetDevice(&tree->device));
+
+  // valid-point compaction (ValidPointIndices, kdtree-impl.h:53-75)
+  DevBuf<int> flag(n + 1, st), off(n + 1, st);
+  int* d_nv_ptr = off.get() + n;
+  if (n > 0) {
+    k_valid<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get());
+    PPTKG_CHECK_LAUNCH();
+  }
+  exclusive_scan<int, int>(flag.get(), off.get(), n, d_nv_ptr, st);
+  int nv = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&nv, d_nv_ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  tree->nv = nv;
+
+  DevBuf<T> xs((size_t)D * nv + 1, st);
+  DevBuf<int> ids(nv + 1, st);
+  SoA<T, D> soa;
+  for (int d = 0; d < D; d++) soa.x[d] = xs.get() + (size_t)d * nv;
+  soa.id = ids.get();
+  if (n > 0) {
+    k_compact<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get(), off.get(), soa);
+    PPTKG_CHECK_LAUNCH();
+  }
+  flag.release();
+  off.release();
+
+  int cap_list;
+  size_t smem;
+  const int small_cap = small_capacity<T, D>(max_leaf, cap_list, smem);
+
+  // records: every node is a disjoint range at its level; nodes with children
+  // have > max_leaf points, so the count is below 2 * nv / (max_leaf + 1) + depth.
+  // every record is a non-empty range and every split has two children, so a
+  // binary tree over nv points has at most 2 * nv - 1 records
+  const size_t rec_cap = 2 * (size_t)nv + 64;
+  DevBuf<Rec<T, D>> recbuf(rec_cap, st);
+  Rec<T, D>* recs = recbuf.get();
+
+  DevBuf<BuildCtl> ctl(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(BuildCtl), st));
+  BuildCtl hctl;
+
+  Seg<T, D> root;
+  memset(&root, 0, sizeof(root));
+  root.b = 0;
+  root.e = nv;
+  root.parent = -1;
+  root.side = 0;
+  root.lvl = 0;
+  for (int d = 0; d < D; d++) {
+    root.lo[d] = Limits<T>::max();  // replaced by the tight box at the root
+    root.hi[d] = Limits<T>::lowest();
+  }
+
+  size_t small_cap_n = 1024;
+  DevBuf<Seg<T, D>> smallL(small_cap_n, st);
+  int nSmall = 0;
+  int depth = 0;
+  if (nv > 0) {
+    if (nv > small_cap) {
+      DevBuf<Seg<T, D>> segA(1, st), segB;
+      PPTKG_CUDA(cudaMemcpyAsync(segA.get(), &root, sizeof(root), cudaMemcpyHostToDevice, st));
+      int nA = 1;
+      int rec_base = 0;
+      DevBuf<int> blpos(nv, st), grpos(nv, st);
+      size_t tile_cap = 0;
+      DevBuf<int> tile_seg;
+      DevBuf<long long> tile_cnt, tile_off;
+      int lvl = 0;
+      while (nA > 0) {
+        const size_t max_tiles = (size_t)nv / TILE + (size_t)nA + 1;
+        if (max_tiles > tile_cap) {
+          tile_cap = max_tiles * 2;
+          tile_seg.alloc(tile_cap, st);
+          tile_cnt.alloc(tile_cap, st);
+          tile_off.alloc(tile_cap, st);
+        }
+        if ((size_t)nSmall + 2 * (size_t)nA > small_cap_n) {
+          size_t nc = std::max(small_cap_n * 2, (size_t)nSmall + 2 * (size_t)nA);
+          DevBuf<Seg<T, D>> bigger(nc, st);
+          if (nSmall)
+            PPTKG_CUDA(cudaMemcpyAsync(bigger.get(), smallL.get(), nSmall * sizeof(Seg<T, D>),
+                                       cudaMemcpyDeviceToDevice, st));
+          std::swap(bigger.p, smallL.p);
+          std::swap(bigger.n, smallL.n);
+          small_cap_n = nc;
+        }
+        segB.alloc(2 * (size_t)nA, st);
+        const unsigned gt = (unsigned)max_tiles;
+        k_tiles<T, D><<<1, 1024, 0, st>>>(segA.get(), nA, tile_seg.get(), ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        k_seg_init<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA);
+        PPTKG_CHECK_LAUNCH();
+        k_bbox<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa);
+        PPTKG_CHECK_LAUNCH();
+        k_node<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA, rec_base, recs, (long long)n, max_leaf, thr);
+        PPTKG_CHECK_LAUNCH();
+        k_count<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa);
+        PPTKG_CHECK_LAUNCH();
+        for (int pass = 1; pass <= 2; pass++) {
+          k_flags<T, D><<<gt, BT, 0, st>>>(pass, segA.get(), tile_seg.get(), ctl.get(), soa, tile_cnt.get());
+          PPTKG_CHECK_LAUNCH();
+          k_tscan<T, D><<<nA, 256, 0, st>>>(segA.get(), tile_cnt.get(), tile_off.get(), ctl.get());
+          PPTKG_CHECK_LAUNCH();
+          k_scatter<T, D><<<gt, BT, 0, st>>>(pass, segA.get(), tile_seg.get(), ctl.get(), soa, tile_off.get(),
+                                            blpos.get(), grpos.get());
+          PPTKG_CHECK_LAUNCH();
+          k_swap<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa, blpos.get(), grpos.get());
+          PPTKG_CHECK_LAUNCH();
+        }
+        PPTKG_CUDA(cudaMemsetAsync(&ctl.get()->nB, 0, sizeof(int), st));
+        k_children<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA, recs, segB.get(), smallL.get(), small_cap,
+                                                          ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        PPTKG_CUDA(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(BuildCtl), cudaMemcpyDeviceToHost, st));
+        PPTKG_CUDA(cudaStreamSynchronize(st));
+        if (hctl.status) throw Error(E_DEVICE, "device build: partition check failed");
+        rec_base += nA;
+        nSmall = hctl.nSmall;
+        nA = hctl.nB;
+        if (lvl > nv) throw Error(E_DEVICE, "device build: level count exceeds the point count");
+        std::swap(segA.p, segB.p);
+        std::swap(segA.n, segB.n);
+        lvl++;
+      }
+      depth = lvl;
+      PPTKG_CUDA(cudaMemcpyAsync(&ctl.get()->rec_count, &rec_base, sizeof(int), cudaMemcpyHostToDevice, st));
+    } else {
+      PPTKG_CUDA(cudaMemcpyAsync(smallL.get(), &root, sizeof(root), cudaMemcpyHostToDevice, st));
+      nSmall = 1;
+    }
+    if (nSmall > 0) {
+      PPTKG_CUDA(cudaFuncSetAttribute(k_subtree<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_subtree<T, D><<<nSmall, SUB_THREADS, smem, st>>>(smallL.get(), soa, recs, small_cap, cap_list, (long long)n,
+                                                         max_leaf, thr, (int)rec_cap, ctl.get());
+      PPTKG_CHECK_LAUNCH();
+    }
+    PPTKG_CUDA(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(BuildCtl), cudaMemcpyDeviceToHost, st));
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+    if (hctl.status) throw Error(E_DEVICE, "device build: subtree check failed (code " + std::to_string(hctl.status) + ")");
+    if ((size_t)hctl.rec_count > rec_cap) throw Error(E_DEVICE, "device build: record capacity exceeded");
+    tree->n_recs = hctl.rec_count;
+    depth = std::max(depth, hctl.depth);
+  }
+  tree->depth = depth;
+  PPTKG_CUDA(cudaMalloc(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>)));
+  if (tree->n_recs)
+    PPTKG_CUDA(cudaMemcpyAsync(tree->recs, recs, tree->n_recs * sizeof(Rec<T, D>), cudaMemcpyDeviceToDevice, st));
+  recs = (Rec<T, D>*)tree->recs;
+  recbuf.release();
+
+  // tree-ordered points and the forward map
+  PointRec<T, D>* pts = nullptr;
+  PPTKG_CUDA(cudaMalloc(&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>)));
+  tree->pts = pts;
+  PPTKG_CUDA(cudaMalloc(&tree->fwd, std::max<int64_t>(n, 1) * sizeof(int)));
+  if (n > 0) PPTKG_CUDA(cudaMemsetAsync(tree->fwd, 0xff, n * sizeof(int), st));
+  if (nv > 0) {
+    k_finish<T, D><<<div_up(nv, 256), 256, 0, st>>>(soa, nv, pts, tree->fwd);
+    PPTKG_CHECK_LAUNCH();
+  }
+
+  // traversal hierarchy cut at `bucket` points
+  make_tnodes<T, D>(tree.get(), bucket, st);
+
+  if (nv > 0) {
+    Rec<T, D> r0;
+    PPTKG_CUDA(cudaMemcpyAsync(&r0, recs, sizeof(r0), cudaMemcpyDeviceToHost, st));
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+    for (int d = 0; d < D; d++) {
+      tree->root_lo[d] = (double)r0.lo[d];
+      tree->root_hi[d] = (double)r0.hi[d];
+    }
+  } else {
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+  }
+  return tree.release();
+}
+
+template <typename T, int D>
+void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
+  if (tree->tnodes) {
+    PPTKG_CUDA(cudaFree(tree->tnodes));
+    tree->tnodes = nullptr;
+  }
+  if (bucket < 1) bucket = 1;
+  tree->bucket = bucket;
+  const int nr = tree->n_recs;
+  const Rec<T, D>* recs = (const Rec<T, D>*)tree->recs;
+  DevBuf<int> flag(nr + 1, st), tid(nr + 1, st);
+  int nt = 0;
+  if (nr > 0) {
+    k_tflag<T, D><<<div_up(nr, 256), 256, 0, st>>>(recs, nr, bucket, flag.get());
+    PPTKG_CHECK_LAUNCH();
+    exclusive_scan<int, int>(flag.get(), tid.get(), nr, tid.get() + nr, st);
+    PPTKG_CUDA(cudaMemcpyAsync(&nt, tid.get() + nr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+  }
+  TNode<T, D>* nodes = nullptr;
+  PPTKG_CUDA(cudaMalloc(&nodes, std::max(nt, 1) * sizeof(TNode<T, D>)));
+  tree->tnodes = nodes;
+  tree->n_tnodes = std::max(nt, 1);
+  if (nt > 0) {
+    k_tfill<T, D><<<div_up(nr, 256), 256, 0, st>>>(recs, nr, flag.get(), tid.get(), nodes);
+  } else {
+    k_tsingle<T, D><<<1, 1, 0, st>>>(recs, nr, (int)tree->nv, nodes);
+  }
+  PPTKG_CHECK_LAUNCH();
+  tree->tdepth = tree->depth + 2;
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+}
+
+size_t TreeBase::device_bytes() const {
+  size_t ps = (dtype == F64 ? 8 : 4) * dim + 4;
+  ps = (ps + 15) / 16 * 16;
+  return ps * nv + 4 * n;
+}
+
+TreeBase::~TreeBase() {
+  if (pts) cudaFree(pts);
+  if (recs) cudaFree(recs);
+  if (tnodes) cudaFree(tnodes);
+  if (fwd) cudaFree(fwd);
+}
+
+#define PPTKG_INST_BUILD(T, D)                                                                         \
+  template TreeBase* build_tree<T, D>(const T*, int64_t, int, double, int, cudaStream_t);             \
+  template void make_tnodes<T, D>(TreeBase*, int, cudaStream_t);
+
+PPTKG_INST_BUILD(float, 3)
+PPTKG_INST_BUILD(double, 3)
+PPTKG_INST_BUILD(float, 2)
+PPTKG_INST_BUILD(double, 2)
+PPTKG_INST_BUILD(float, 4)
+PPTKG_INST_BUILD(double, 4)
+
+}  // namespace pptkg

@@ -1,0 +1,26 @@
+// Device k-d tree builder (exact replica of the reference tree).
+#pragma once
+
+#include <memory>
+
+#include "tree.cuh"
+
+namespace pptkg {
+
+// Working structure-of-arrays copy of the valid points during the build.
+template <typename T, int D>
+struct SoA {
+  T* x[D];
+  int* id;
+};
+
+// Builds the tree over n contiguous AoS points already on the device.
+// Rows with a NaN/inf coordinate are dropped, as in the reference.
+template <typename T, int D>
+TreeBase* build_tree(const T* d_points, int64_t n, int max_leaf, double empty_split, int bucket, cudaStream_t st);
+
+// (Re)derives the traversal hierarchy for a bucket size.
+template <typename T, int D>
+void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st);
+
+}  // namespace pptkg

@@ -1,0 +1,117 @@
+// Shared device helpers for the pptk B200 kernels: element-type traits,
+// reference-exact arithmetic (no FMA contraction), ordered integer images of
+// floating point values for atomic min/max, and error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cfloat>
+#include <climits>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace pptkg {
+
+// ---------------------------------------------------------------- errors --
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+enum Status {
+  OK = 0,
+  E_INVALID = 1,     // bad argument (ValueError at the Python boundary)
+  E_TYPE = 2,        // unsupported dtype / dim (TypeError)
+  E_CUDA = 3,        // CUDA runtime failure
+  E_RANGE = 4,       // index outside the point range (RuntimeError)
+  E_DEVICE = 5,      // a kernel reported a failed internal check
+  E_UNSUPPORTED = 6  // NotImplementedError
+};
+
+#define PPTKG_CUDA(call)                                                                        \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      throw ::pptkg::Error(::pptkg::E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Counts every kernel launch of the library (pptkg_launch_count) and checks it.
+extern std::atomic<long long> g_launches;
+#define PPTKG_CHECK_LAUNCH()          \
+  do {                                \
+    ::pptkg::g_launches++;            \
+    PPTKG_CUDA(cudaGetLastError());   \
+  } while (0)
+
+// ------------------------------------------------------------ dtype codes --
+// Identical to include/pptkg.h.
+enum DType { F32 = 0, F64 = 1, I8 = 2, I16 = 3, I32 = 4, I64 = 5, U8 = 6, U16 = 7, U32 = 8, U64 = 9 };
+
+inline int dtype_size(int dt) {
+  switch (dt) {
+    case F32: case I32: case U32: return 4;
+    case F64: case I64: case U64: return 8;
+    case I16: case U16: return 2;
+    case I8: case U8: return 1;
+  }
+  return 0;
+}
+
+// Distance arithmetic type: float for float32 and all integer types, double
+// for float64 (pptk/kdtree/src/accumulator.h:13-27).
+template <typename T> struct DistOf { typedef float type; };
+template <> struct DistOf<double> { typedef double type; };
+
+template <typename T> struct Limits;
+template <> struct Limits<float> {
+  __host__ __device__ static float max() { return FLT_MAX; }
+  __host__ __device__ static float lowest() { return -FLT_MAX; }
+};
+template <> struct Limits<double> {
+  __host__ __device__ static double max() { return DBL_MAX; }
+  __host__ __device__ static double lowest() { return -DBL_MAX; }
+};
+
+// --------------------------------------------- exact (uncontracted) math --
+// Every operation below rounds once, as the reference's x86-64 SSE build does
+// (no -march, hence no FMA; pptk CMakeLists.txt:4).
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// ------------------------------------------ ordered integer images (min/max)
+// Monotone map from a float/double to an unsigned integer so that atomicMin /
+// atomicMax on the image order like the values (NaN excluded; -0 < +0).
+__host__ __device__ __forceinline__ uint32_t ord_of(float f) {
+  uint32_t u = *reinterpret_cast<uint32_t*>(&f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float from_ord(uint32_t u) {
+  u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  return *reinterpret_cast<float*>(&u);
+}
+__host__ __device__ __forceinline__ unsigned long long ord_of(double f) {
+  unsigned long long u = *reinterpret_cast<unsigned long long*>(&f);
+  return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
+  u = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+  return *reinterpret_cast<double*>(&u);
+}
+
+template <typename T> struct OrdOf;
+template <> struct OrdOf<float> { typedef uint32_t type; };
+template <> struct OrdOf<double> { typedef unsigned long long type; };
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+__host__ __device__ __forceinline__ int div_up_dev(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace pptkg

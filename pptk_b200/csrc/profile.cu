@@ -1,0 +1,73 @@
+// Stage timing store behind pptkg_profile_enable / pptkg_profile_get.
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "pptkg.h"
+#include "profile.cuh"
+
+namespace pptkg {
+
+std::atomic<long long> g_launches{0};
+
+namespace {
+struct Pending {
+  std::string name;
+  cudaEvent_t a, b;
+};
+std::mutex g_mu;
+bool g_on = false;
+std::vector<Pending> g_pending;
+std::map<std::string, std::pair<double, long long>> g_total;
+
+void drain_locked() {
+  for (auto& p : g_pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      auto& t = g_total[p.name];
+      t.first += ms;
+      t.second += 1;
+    }
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  g_pending.clear();
+}
+}  // namespace
+
+bool profiling_on() {
+  std::lock_guard<std::mutex> g(g_mu);
+  return g_on;
+}
+
+void profile_record(const char* stage, cudaEvent_t a, cudaEvent_t b) {
+  std::lock_guard<std::mutex> g(g_mu);
+  g_pending.push_back({stage, a, b});
+}
+
+}  // namespace pptkg
+
+extern "C" {
+
+int pptkg_profile_enable(int on) {
+  std::lock_guard<std::mutex> g(pptkg::g_mu);
+  pptkg::drain_locked();
+  pptkg::g_total.clear();
+  pptkg::g_on = on != 0;
+  return PPTKG_OK;
+}
+
+int pptkg_profile_get(const char* stage, double* total_ms, int64_t* count) {
+  std::lock_guard<std::mutex> g(pptkg::g_mu);
+  pptkg::drain_locked();
+  auto it = pptkg::g_total.find(stage ? stage : "");
+  if (total_ms) *total_ms = it == pptkg::g_total.end() ? 0.0 : it->second.first;
+  if (count) *count = it == pptkg::g_total.end() ? 0 : it->second.second;
+  return PPTKG_OK;
+}
+
+int64_t pptkg_launch_count(void) { return pptkg::g_launches.load(); }
+
+}  // extern "C"

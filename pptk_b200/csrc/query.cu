@@ -1,0 +1,721 @@
+// Query kernels: exact kNN (point and self forms), r-near count/fill in the
+// reference's order, and fused kNN + PCA normal estimation.
+#include <algorithm>
+
+#include "knn.cuh"
+#include "normals.cuh"
+#include "profile.cuh"
+#include "query.cuh"
+#include "util.cuh"
+
+namespace pptkg {
+
+constexpr int QWARPS = 4;
+constexpr int QTHREADS = QWARPS * 32;
+
+template <typename T, int D>
+TreeView<T, D> view_of(const TreeBase* t) {
+  TreeView<T, D> v;
+  v.pts = (const PointRec<T, D>*)t->pts;
+  v.nodes = (const TNode<T, D>*)t->tnodes;
+  v.nv = (int)t->nv;
+  v.depth = t->tdepth;
+  v.n_nodes = t->n_tnodes;
+  return v;
+}
+
+template <typename T, int D>
+size_t warp_smem_bytes(int depth) {
+  return 32 * sizeof(PointRec<T, D>) + (((size_t)depth * 4 + 15) & ~(size_t)15);
+}
+
+template <typename T, int D>
+__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth) {
+  extern __shared__ __align__(16) unsigned char qsm[];
+  const size_t per = 32 * sizeof(PointRec<T, D>) + (((size_t)depth * 4 + 15) & ~(size_t)15);
+  unsigned char* base = qsm + (threadIdx.x >> 5) * per;
+  WarpScratch<T, D> ws;
+  ws.buf = (PointRec<T, D>*)base;
+  ws.stack = (int*)(base + 32 * sizeof(PointRec<T, D>));
+  return ws;
+}
+
+// ------------------------------------------------------------- loaders ----
+// Query i is row i of a user array.
+template <typename Q, int D>
+struct PointQueries {
+  const Q* q;
+  template <typename T, typename DistT>
+  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own) const {
+#pragma unroll
+    for (int d = 0; d < D; d++) out[d] = (DistT)q[(int64_t)i * D + d];
+    own = -1;
+    return true;
+  }
+};
+
+// Query i is the stored point with original index idx[i] (or i); EXCL drops
+// the point itself from its own result (KNearestNeighborsSelf,
+// kdtree-impl.h:931-948; RNearNeighborsSelf, :1028-1043).
+template <int D, bool EXCL>
+struct IndexQueries {
+  const int* idx;
+  const int* fwd;
+  template <typename T, typename DistT>
+  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own) const {
+    const int o = idx ? idx[i] : i;
+    const int p = fwd[o];
+    own = -1;
+    if (p < 0) return false;  // the point was dropped (NaN/inf): no neighbours
+    const PointRec<T, D> r = tv.pts[p];
+#pragma unroll
+    for (int d = 0; d < D; d++) out[d] = (DistT)r.c[d];
+    own = EXCL ? p : -1;
+    return true;
+  }
+};
+
+// order_mode 0: slot = query; 1: order[slot]; 2: tree order (query = the
+// original index stored at tree position slot).
+template <typename T, int D>
+__device__ __forceinline__ int query_of(int slot, const int* order, int order_mode, const TreeView<T, D>& tv) {
+  return order_mode == 0 ? slot : (order_mode == 1 ? order[slot] : tv.pts[slot].id);
+}
+
+// ----------------------------------------------------------- ordering ----
+template <typename T, int D, typename Q>
+__global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
+  typedef typename DistOf<T>::type DistT;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  DistT p[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) p[d] = (DistT)q[(int64_t)i * D + d];
+  int cur = 0, k = 0;
+  for (int step = 0; step <= tv.depth + 1; step++) {
+    const TNode<T, D>& nd = tv.nodes[cur];
+    int c;
+    if (nd.cnt[1] == 0)
+      c = 0;
+    else if (nd.cnt[0] == 0)
+      c = 1;
+    else
+      c = box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], p) < box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], p);
+    const int ref = nd.ref[c];
+    if (ref < 0) {
+      k = -ref - 1;
+      break;
+    }
+    cur = ref;
+  }
+  key[i] = min(max(k, 0), tv.nv);
+}
+
+__global__ void k_check_idx(const int* idx, int m, int n, int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m && (idx[i] < 0 || idx[i] >= n)) atomicExch(status, 4);
+}
+
+// Rejects index queries outside [0, n) before any kernel dereferences them.
+static void check_indices(const TreeBase* t, const QuerySpec& qs, cudaStream_t st) {
+  if (qs.pts || !qs.idx || qs.m <= 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  k_check_idx<<<div_up(qs.m, 256), 256, 0, st>>>(qs.idx, (int)qs.m, (int)t->n, status.get());
+  PPTKG_CHECK_LAUNCH();
+  int h = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&h, status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h) throw Error(E_RANGE, "query index outside of [0, n)");
+}
+
+__global__ void k_idxkey(const int* idx, const int* fwd, int m, int nv, int* key) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int p = fwd[idx ? idx[i] : i];
+  key[i] = p < 0 ? nv : p;
+}
+
+__global__ void k_hist(const int* key, int m, int* hist) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) atomicAdd(&hist[key[i]], 1);
+}
+
+__global__ void k_place(const int* key, int m, int* cursor, int* order) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) order[atomicAdd(&cursor[key[i]], 1)] = i;
+}
+
+// Builds a processing order in which queries near each other in the tree are
+// adjacent (counting sort on the tree position key).  Returns the order mode.
+template <typename T, int D>
+int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaStream_t st) {
+  check_indices(t, qs, st);
+  Stage stage("order", st);
+  const int m = (int)qs.m;
+  const int nv = (int)t->nv;
+  if (m <= 0) return 0;
+  if (!qs.pts && !qs.idx && m == nv && t->n == t->nv) return 2;  // all points, tree order
+  if (m < 2048) return 0;
+  DevBuf<int> key(m, st), hist(nv + 2, st);
+  if (qs.pts) {
+    if (qs.qdtype == F64)
+      k_locate<T, D, double><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const double*)qs.pts, m, key.get());
+    else
+      k_locate<T, D, float><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const float*)qs.pts, m, key.get());
+  } else {
+    k_idxkey<<<div_up(m, 256), 256, 0, st>>>(qs.idx, t->fwd, m, nv, key.get());
+  }
+  PPTKG_CHECK_LAUNCH();
+  PPTKG_CUDA(cudaMemsetAsync(hist.get(), 0, sizeof(int) * (nv + 2), st));
+  k_hist<<<div_up(m, 256), 256, 0, st>>>(key.get(), m, hist.get());
+  PPTKG_CHECK_LAUNCH();
+  exclusive_scan<int, int>(hist.get(), hist.get(), nv + 1, (int*)nullptr, st);
+  order.alloc(m, st);
+  k_place<<<div_up(m, 256), 256, 0, st>>>(key.get(), m, hist.get(), order.get());
+  PPTKG_CHECK_LAUNCH();
+  return 1;
+}
+
+// ----------------------------------------------------------------- kNN ----
+template <typename T, int D, int KMAX, typename L>
+__global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
+                                                  int k, typename DistOf<T>::type r2, int32_t* out_idx,
+                                                  int32_t* out_cnt, int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int slot = blockIdx.x * QTHREADS + threadIdx.x;
+  if ((slot & ~31) >= m) return;
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
+  int qid = -1, own = -1;
+  DistT q[D];
+  bool active = false;
+  if (slot < m) {
+    qid = query_of(slot, order, order_mode, tv);
+    active = ld.load(qid, tv, q, own);
+  }
+  if (!active)
+#pragma unroll
+    for (int d = 0; d < D; d++) q[d] = (DistT)0;
+  TopK<KMAX, DistT> top;
+  top.reset(k, r2);
+  if (!packet_knn<T, D, KMAX, DistT>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (slot < m) {
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < KMAX; j++) {
+      if (j < k) {
+        const bool v = active && top.valid(j);
+        c += v;
+        out_idx[(int64_t)qid * k + (k - 1 - j)] = v ? tv.pts[top.pos(j)].id : -1;
+      }
+    }
+    if (out_cnt) out_cnt[qid] = c;
+  }
+}
+
+template <typename T, int D, int KMAX, typename L>
+void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st) {
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
+  if (smem > 48 * 1024)
+    PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
+                                                                      d_idx, d_cnt, status);
+  PPTKG_CHECK_LAUNCH();
+}
+
+template <typename T, int D, typename L>
+void dispatch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                  int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st) {
+  if (k <= 4)
+    launch_knn<T, D, 4>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+  else if (k <= 8)
+    launch_knn<T, D, 8>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+  else if (k <= 16)
+    launch_knn<T, D, 16>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+  else if (k <= 32)
+    launch_knn<T, D, 32>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+  else
+    launch_knn<T, D, 64>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+}
+
+template <typename DistT>
+DistT radius2(double dmax) {
+  // the reference casts dmax to the distance type and squares it there
+  // (kdtree_wrapper.cpp:144-146, kdtree-impl.h:881)
+  const DistT r = (DistT)dmax;
+  return r * r;
+}
+
+static void check_status(int* d_status, cudaStream_t st, const char* what) {
+  int h = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h) throw Error(E_DEVICE, std::string(what) + ": device traversal check failed (code " + std::to_string(h) + ")");
+}
+
+template <typename T, int D>
+void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32_t* d_idx, int32_t* d_cnt,
+               cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k < 1) throw Error(E_INVALID, "k must be positive");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU kNN kernels");
+  const int m = (int)qs.m;
+  if (m <= 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  DevBuf<int> order;
+  const int mode = make_order<T, D>(t, qs, order, st);
+  const DistT r2 = radius2<DistT>(dmax);
+  Stage stage("knn", st);
+  if (qs.pts) {
+    if (qs.qdtype == F64)
+      dispatch_knn<T, D>(t, PointQueries<double, D>{(const double*)qs.pts}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                         status.get(), st);
+    else
+      dispatch_knn<T, D>(t, PointQueries<float, D>{(const float*)qs.pts}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                         status.get(), st);
+  } else if (qs.exclude_self) {
+    dispatch_knn<T, D>(t, IndexQueries<D, true>{qs.idx, t->fwd}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                       status.get(), st);
+  } else {
+    dispatch_knn<T, D>(t, IndexQueries<D, false>{qs.idx, t->fwd}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                       status.get(), st);
+  }
+  check_status(status.get(), st, "knn");
+}
+
+// -------------------------------------------------------------- r-near ----
+template <typename T, int D, typename L>
+__global__ void __launch_bounds__(QTHREADS) k_rnear_count(TreeView<T, D> tv, L ld, const int* order, int order_mode,
+                                                          int m, typename DistOf<T>::type r2, int64_t* counts,
+                                                          int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int slot = blockIdx.x * QTHREADS + threadIdx.x;
+  if ((slot & ~31) >= m) return;
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
+  int qid = -1, own = -1;
+  DistT q[D];
+  bool active = false;
+  if (slot < m) {
+    qid = query_of(slot, order, order_mode, tv);
+    active = ld.load(qid, tv, q, own);
+  }
+  if (!active)
+#pragma unroll
+    for (int d = 0; d < D; d++) q[d] = (DistT)0;
+  long long cnt = 0;
+  auto none = [](int, const PointRec<T, D>&) {};
+  if (!packet_rnear<T, D, DistT, true>(tv, q, active, r2, ws, cnt, none)) atomicExch(status, 1);
+  if (own >= 0 && cnt > 0) cnt -= 1;  // the point itself is always a hit when r2 > 0
+  if (slot < m) counts[qid] = active ? cnt : 0;
+}
+
+template <typename T, int D, typename L>
+__global__ void __launch_bounds__(QTHREADS) k_rnear_fill(TreeView<T, D> tv, L ld, const int* order, int order_mode,
+                                                         int m, typename DistOf<T>::type r2, const int64_t* off,
+                                                         int32_t* out, int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int slot = blockIdx.x * QTHREADS + threadIdx.x;
+  if ((slot & ~31) >= m) return;
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
+  int qid = -1, own = -1;
+  DistT q[D];
+  bool active = false;
+  if (slot < m) {
+    qid = query_of(slot, order, order_mode, tv);
+    active = ld.load(qid, tv, q, own);
+  }
+  if (!active)
+#pragma unroll
+    for (int d = 0; d < D; d++) q[d] = (DistT)0;
+  int64_t w = active ? off[qid] : 0;
+  const int64_t wend = active ? off[qid + 1] : 0;
+  bool overflow = false;
+  long long unused = 0;
+  auto emit = [&](int pos, const PointRec<T, D>& pr) {
+    if (pos == own) return;
+    if (w < wend)
+      out[w++] = pr.id;
+    else
+      overflow = true;
+  };
+  if (!packet_rnear<T, D, DistT, false>(tv, q, active, r2, ws, unused, emit)) atomicExch(status, 1);
+  if (overflow || w != wend) atomicExch(status, 2);
+}
+
+template <typename T, int D, typename F>
+void with_loader(const TreeBase* t, const QuerySpec& qs, F&& f) {
+  if (qs.pts) {
+    if (qs.qdtype == F64)
+      f(PointQueries<double, D>{(const double*)qs.pts});
+    else
+      f(PointQueries<float, D>{(const float*)qs.pts});
+  } else if (qs.exclude_self) {
+    f(IndexQueries<D, true>{qs.idx, t->fwd});
+  } else {
+    f(IndexQueries<D, false>{qs.idx, t->fwd});
+  }
+}
+
+template <typename T, int D>
+int64_t rnear_count(const TreeBase* t, const QuerySpec& qs, double dmax, int64_t* d_off, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  const int m = (int)qs.m;
+  if (m <= 0) {
+    PPTKG_CUDA(cudaMemsetAsync(d_off, 0, sizeof(int64_t), st));
+    return 0;
+  }
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  DevBuf<int> order;
+  const int mode = make_order<T, D>(t, qs, order, st);
+  const DistT r2 = radius2<DistT>(dmax);
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
+  Stage stage("rnear_count", st);
+  with_loader<T, D>(t, qs, [&](auto ld) {
+    typedef decltype(ld) L;
+    if (smem > 48 * 1024)
+      PPTKG_CUDA(cudaFuncSetAttribute(k_rnear_count<T, D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rnear_count<T, D, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order.get(), mode, m,
+                                                                          r2, d_off, status.get());
+    PPTKG_CHECK_LAUNCH();
+  });
+  exclusive_scan<int64_t, int64_t>(d_off, d_off, m, d_off + m, st);
+  check_status(status.get(), st, "rnear_count");
+  int64_t total = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&total, d_off + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  return total;
+}
+
+template <typename T, int D>
+void rnear_fill(const TreeBase* t, const QuerySpec& qs, double dmax, const int64_t* d_off, int32_t* d_out,
+                cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  const int m = (int)qs.m;
+  if (m <= 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  DevBuf<int> order;
+  const int mode = make_order<T, D>(t, qs, order, st);
+  const DistT r2 = radius2<DistT>(dmax);
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
+  Stage stage("rnear_fill", st);
+  with_loader<T, D>(t, qs, [&](auto ld) {
+    typedef decltype(ld) L;
+    if (smem > 48 * 1024)
+      PPTKG_CUDA(cudaFuncSetAttribute(k_rnear_fill<T, D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rnear_fill<T, D, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order.get(), mode, m, r2,
+                                                                         d_off, d_out, status.get());
+    PPTKG_CHECK_LAUNCH();
+  });
+  check_status(status.get(), st, "rnear_fill");
+}
+
+// ------------------------------------------------------------- normals ----
+// Covariance of the neighbourhood in precision P, each neighbour shifted to
+// the query point first (p - q, formed in the input type's precision or
+// better), then mean-centred in a second pass with compensated sums.
+template <typename T, typename P, int KMAX, typename DistT>
+__device__ __forceinline__ Sym3<P> knn_covariance(const TreeView<T, 3>& tv, const TopK<KMAX, DistT>& top, int k,
+                                                  const DistT* q, int& n) {
+  typedef typename std::conditional<(sizeof(T) > sizeof(P)), T, P>::type W;
+  P s0 = 0, s1 = 0, s2 = 0;
+  n = 0;
+#pragma unroll
+  for (int j = 0; j < KMAX; j++) {
+    if (j < k && top.valid(j)) {
+      const PointRec<T, 3> r = tv.pts[top.pos(j)];
+      s0 += (P)((W)r.c[0] - (W)q[0]);
+      s1 += (P)((W)r.c[1] - (W)q[1]);
+      s2 += (P)((W)r.c[2] - (W)q[2]);
+      n++;
+    }
+  }
+  const P inv = n > 0 ? (P)1 / (P)n : (P)0;
+  const P m0 = s0 * inv, m1 = s1 * inv, m2 = s2 * inv;
+  CSum<P> c00, c01, c02, c11, c12, c22;
+#pragma unroll
+  for (int j = 0; j < KMAX; j++) {
+    if (j < k && top.valid(j)) {
+      const PointRec<T, 3> r = tv.pts[top.pos(j)];
+      const P e0 = (P)((W)r.c[0] - (W)q[0]) - m0;
+      const P e1 = (P)((W)r.c[1] - (W)q[1]) - m1;
+      const P e2 = (P)((W)r.c[2] - (W)q[2]) - m2;
+      c00.add(e0 * e0);
+      c01.add(e0 * e1);
+      c02.add(e0 * e2);
+      c11.add(e1 * e1);
+      c12.add(e1 * e2);
+      c22.add(e2 * e2);
+    }
+  }
+  Sym3<P> C;
+  C.a00 = c00.value() * inv;
+  C.a01 = c01.value() * inv;
+  C.a02 = c02.value() * inv;
+  C.a11 = c11.value() * inv;
+  C.a12 = c12.value() * inv;
+  C.a22 = c22.value() * inv;
+  return C;
+}
+
+template <typename T, typename P>
+__device__ __forceinline__ void write_pca(int row, int n, const P w[3], const P V[9], int num_eigen, T* evecs, T* evals,
+                                          int32_t* sizes) {
+  if (num_eigen == 1) {
+    if (evecs) {
+      evecs[(int64_t)row * 3 + 0] = (T)V[0];
+      evecs[(int64_t)row * 3 + 1] = (T)V[3];
+      evecs[(int64_t)row * 3 + 2] = (T)V[6];
+    }
+    if (evals) evals[row] = (T)w[0];
+  } else {
+    if (evecs)
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) evecs[(int64_t)row * 9 + e * 3 + c] = (T)V[c * 3 + e];
+    if (evals)
+#pragma unroll
+      for (int e = 0; e < 3; e++) evals[(int64_t)row * 3 + e] = (T)w[e];
+  }
+  if (sizes) sizes[row] = n;
+}
+
+template <typename T>
+__device__ __forceinline__ void write_invalid(int row, int num_eigen, T* evecs, T* evals, int32_t* sizes) {
+  const T nan = (T)NAN;
+  const int nv = num_eigen == 1 ? 3 : 9;
+  if (evecs)
+    for (int c = 0; c < nv; c++) evecs[(int64_t)row * nv + c] = nan;
+  if (evals)
+    for (int c = 0; c < num_eigen; c++) evals[(int64_t)row * num_eigen + c] = nan;
+  if (sizes) sizes[row] = 0;
+}
+
+template <typename T, int KMAX, typename L, int PREC>
+__global__ void __launch_bounds__(QTHREADS) k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
+                                                      int k, typename DistOf<T>::type r2, int num_eigen,
+                                                      double gap_thr, T* evecs, T* evals, int32_t* sizes,
+                                                      int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int slot = blockIdx.x * QTHREADS + threadIdx.x;
+  if ((slot & ~31) >= m) return;
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth);
+  int qid = -1, own = -1;
+  DistT q[3];
+  bool active = false;
+  if (slot < m) {
+    qid = query_of(slot, order, order_mode, tv);
+    active = ld.load(qid, tv, q, own);
+  }
+  if (!active) q[0] = q[1] = q[2] = (DistT)0;
+  TopK<KMAX, DistT> top;
+  top.reset(k, r2);
+  if (!packet_knn<T, 3, KMAX, DistT>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (slot >= m) return;
+  if (!active) {
+    write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
+    return;
+  }
+  int n;
+  if (PREC == PREC_FP64) {
+    Sym3<double> C = knn_covariance<T, double, KMAX, DistT>(tv, top, k, q, n);
+    double w[3], V[9];
+    eigh3<double>(C, w, V);
+    write_pca<T, double>(qid, n, w, V, num_eigen, evecs, evals, sizes);
+  } else {
+    Sym3<float> C = knn_covariance<T, float, KMAX, DistT>(tv, top, k, q, n);
+    float w[3], V[9];
+    eigh3<float>(C, w, V);
+    if (!(rel_gap<float>(w) >= (float)gap_thr)) {
+      // small eigen-gap: the normal direction is ill-conditioned in FP32;
+      // redo this neighbourhood in FP64
+      Sym3<double> Cd = knn_covariance<T, double, KMAX, DistT>(tv, top, k, q, n);
+      double wd[3], Vd[9];
+      eigh3<double>(Cd, wd, Vd);
+      write_pca<T, double>(qid, n, wd, Vd, num_eigen, evecs, evals, sizes);
+      return;
+    }
+    write_pca<T, float>(qid, n, w, V, num_eigen, evecs, evals, sizes);
+  }
+}
+
+// r-near neighbourhoods (k == -1): moments accumulated during the traversal
+// in FP64, shifted to the query point.
+template <typename T, typename L>
+__global__ void __launch_bounds__(QTHREADS) k_normals_rnear(TreeView<T, 3> tv, L ld, const int* order, int order_mode,
+                                                            int m, typename DistOf<T>::type r2, int num_eigen,
+                                                            T* evecs, T* evals, int32_t* sizes, int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int slot = blockIdx.x * QTHREADS + threadIdx.x;
+  if ((slot & ~31) >= m) return;
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth);
+  int qid = -1, own = -1;
+  DistT q[3];
+  bool active = false;
+  if (slot < m) {
+    qid = query_of(slot, order, order_mode, tv);
+    active = ld.load(qid, tv, q, own);
+  }
+  if (!active) q[0] = q[1] = q[2] = (DistT)0;
+  double s[3] = {0, 0, 0}, ss[6] = {0, 0, 0, 0, 0, 0};
+  long long n = 0;
+  auto emit = [&](int pos, const PointRec<T, 3>& pr) {
+    const double e0 = (double)pr.c[0] - (double)q[0], e1 = (double)pr.c[1] - (double)q[1],
+                 e2 = (double)pr.c[2] - (double)q[2];
+    s[0] += e0;
+    s[1] += e1;
+    s[2] += e2;
+    ss[0] += e0 * e0;
+    ss[1] += e0 * e1;
+    ss[2] += e0 * e2;
+    ss[3] += e1 * e1;
+    ss[4] += e1 * e2;
+    ss[5] += e2 * e2;
+    n++;
+  };
+  long long unused = 0;
+  if (!packet_rnear<T, 3, DistT, false>(tv, q, active, r2, ws, unused, emit)) atomicExch(status, 1);
+  if (slot >= m) return;
+  if (!active || n == 0) {
+    write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
+    return;
+  }
+  const double inv = 1.0 / (double)n;
+  const double m0 = s[0] * inv, m1 = s[1] * inv, m2 = s[2] * inv;
+  Sym3<double> C;
+  C.a00 = ss[0] * inv - m0 * m0;
+  C.a01 = ss[1] * inv - m0 * m1;
+  C.a02 = ss[2] * inv - m0 * m2;
+  C.a11 = ss[3] * inv - m1 * m1;
+  C.a12 = ss[4] * inv - m1 * m2;
+  C.a22 = ss[5] * inv - m2 * m2;
+  double w[3], V[9];
+  eigh3<double>(C, w, V);
+  write_pca<T, double>(qid, (int)n, w, V, num_eigen, evecs, evals, sizes);
+}
+
+template <typename T, int KMAX, typename L, int PREC>
+void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                    int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st) {
+  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth);
+  if (smem > 48 * 1024)
+    PPTKG_CUDA(
+        cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, 3>(t), ld, order, mode, m, k, r2,
+                                                                             num_eigen, gap_thr, ev, ew, sz, status);
+  PPTKG_CHECK_LAUNCH();
+}
+
+template <typename T, typename L, int PREC>
+void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k,
+                      typename DistOf<T>::type r2, int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz,
+                      int* status, cudaStream_t st) {
+  if (k <= 4)
+    launch_normals<T, 4, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+  else if (k <= 8)
+    launch_normals<T, 8, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+  else if (k <= 16)
+    launch_normals<T, 16, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+  else if (k <= 32)
+    launch_normals<T, 32, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+  else
+    launch_normals<T, 64, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+}
+
+template <typename T>
+void normals_query(const TreeBase* t, const QuerySpec& qs_in, int k, float r, int num_eigen, int precision,
+                   double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k == 0 || k < -1) throw Error(E_INVALID, "k must be positive or -1");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU normal kernels");
+  QuerySpec qs = qs_in;
+  qs.pts = nullptr;
+  qs.exclude_self = false;
+  const int m = (int)qs.m;
+  if (m <= 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  DevBuf<int> order;
+  int mode = make_order<T, 3>(t, qs, order, st);
+  if (mode == 2) {
+    // tree order covers valid points only: rows of dropped points (none when
+    // n == nv) need no separate pass
+  }
+  // the radius travels as a C float (estimate_normals.cpp:264) and is cast to
+  // the input type (:17-22) before being squared in the distance type
+  const DistT rr = (DistT)(T)r;
+  const DistT r2 = rr * rr;
+  IndexQueries<3, false> ld{qs.idx, t->fwd};
+  Stage stage("normals", st);
+  if (k == -1) {
+    const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth);
+    if (smem > 48 * 1024)
+      PPTKG_CUDA(cudaFuncSetAttribute(k_normals_rnear<T, IndexQueries<3, false>>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_normals_rnear<T, IndexQueries<3, false>><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
+        view_of<T, 3>(t), ld, order.get(), mode, m, r2, num_eigen, d_evecs, d_evals, d_sizes, status.get());
+    PPTKG_CHECK_LAUNCH();
+  } else {
+    int prec = precision;
+    if (prec == PREC_AUTO) prec = sizeof(T) == 4 ? PREC_FP32 : PREC_FP64;
+    if (prec == PREC_FP64)
+      dispatch_normals<T, IndexQueries<3, false>, PREC_FP64>(t, ld, order.get(), mode, m, k, r2, num_eigen, gap_thr,
+                                                             d_evecs, d_evals, d_sizes, status.get(), st);
+    else
+      dispatch_normals<T, IndexQueries<3, false>, PREC_FP32>(t, ld, order.get(), mode, m, k, r2, num_eigen, gap_thr,
+                                                             d_evecs, d_evals, d_sizes, status.get(), st);
+  }
+  check_status(status.get(), st, "normals");
+}
+
+// --------------------------------------------------------------- eigh3 ----
+template <typename T>
+__global__ void k_eigh3(const T* A, int64_t m, T* w, T* V, int layout) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const T* a = A + i * 9;
+  Sym3<T> S;
+  S.a00 = a[0];
+  S.a01 = a[1];
+  S.a02 = a[2];
+  S.a11 = a[4];
+  S.a12 = a[5];
+  S.a22 = a[8];
+  T ww[3], VV[9];
+  eigh3<T>(S, ww, VV);
+  for (int e = 0; e < 3; e++) w[i * 3 + e] = ww[e];
+  // layout 0: V[i, r, c] = component r of eigenvector c (columns, as
+  // vfuncs._eigh returns them); layout 1: [i, e, :] = eigenvector e
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) V[i * 9 + r * 3 + c] = layout == 0 ? VV[r * 3 + c] : VV[c * 3 + r];
+}
+
+template <typename T>
+void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStream_t st) {
+  if (m <= 0) return;
+  k_eigh3<T><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(d_A, m, d_w, d_V, layout);
+  PPTKG_CHECK_LAUNCH();
+}
+
+#define PPTKG_INST_Q(T, D)                                                                                 \
+  template void knn_query<T, D>(const TreeBase*, const QuerySpec&, int, double, int32_t*, int32_t*,        \
+                                cudaStream_t);                                                             \
+  template int64_t rnear_count<T, D>(const TreeBase*, const QuerySpec&, double, int64_t*, cudaStream_t);   \
+  template void rnear_fill<T, D>(const TreeBase*, const QuerySpec&, double, const int64_t*, int32_t*,      \
+                                 cudaStream_t);
+
+PPTKG_INST_Q(float, 3)
+PPTKG_INST_Q(double, 3)
+
+template void normals_query<float>(const TreeBase*, const QuerySpec&, int, float, int, int, double, float*, float*,
+                                   int32_t*, cudaStream_t);
+template void normals_query<double>(const TreeBase*, const QuerySpec&, int, float, int, int, double, double*, double*,
+                                    int32_t*, cudaStream_t);
+template void eigh3_batched<float>(const float*, int64_t, float*, float*, int, cudaStream_t);
+template void eigh3_batched<double>(const double*, int64_t, double*, double*, int, cudaStream_t);
+
+}  // namespace pptkg

@@ -1,0 +1,48 @@
+// Host entry points of the query kernels (kNN, r-near, normals).
+#pragma once
+
+#include "tree.cuh"
+
+namespace pptkg {
+
+// Which points a query batch asks about.
+struct QuerySpec {
+  // point queries: m rows of `dim` coordinates of qdtype (F32 or F64), device
+  const void* pts = nullptr;
+  int qdtype = F32;
+  // index queries: original point indices (device), or all of [0, m) when null
+  const int32_t* idx = nullptr;
+  int64_t m = 0;
+  // index queries exclude the query point itself (the reference's *Self forms)
+  bool exclude_self = true;
+};
+
+constexpr int KNN_MAX_K = 64;
+
+template <typename T, int D>
+void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32_t* d_idx, int32_t* d_cnt,
+               cudaStream_t st);
+
+// Writes per-query hit counts into d_off[0..m) and turns them into offsets
+// (d_off has m + 1 entries); returns the total.
+template <typename T, int D>
+int64_t rnear_count(const TreeBase* t, const QuerySpec& qs, double dmax, int64_t* d_off, cudaStream_t st);
+
+template <typename T, int D>
+void rnear_fill(const TreeBase* t, const QuerySpec& qs, double dmax, const int64_t* d_off, int32_t* d_out,
+                cudaStream_t st);
+
+enum Precision { PREC_AUTO = 0, PREC_FP32 = 1, PREC_FP64 = 2 };
+
+// PCA normals of the points with original indices qs.idx (or all n points)
+// over their k nearest neighbours including themselves (k == -1: r-near
+// neighbourhoods).  Outputs are indexed by query row; any may be null.
+template <typename T>
+void normals_query(const TreeBase* t, const QuerySpec& qs, int k, float r, int num_eigen, int precision,
+                   double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st);
+
+// Batched symmetric 3x3 eigensolve (row-major inputs).
+template <typename T>
+void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStream_t st);
+
+}  // namespace pptkg

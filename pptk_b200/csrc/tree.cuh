@@ -1,0 +1,80 @@
+// Device-resident k-d tree layout.
+//
+// The build reproduces the reference tree exactly (pptk/kdtree/src/
+// kdtree-impl.h:248-329, 773-818): the same point permutation, the same
+// split and empty-split ("trim") nodes.  It leaves three products in HBM:
+//
+//  * PointRec[nv]  -- the valid points in tree order, each with its original
+//                     index (the reference's points_ + reverse_indices_,
+//                     kdtree.h:236-248), 16 B for float32 xyz;
+//  * Rec[n_recs]   -- one record per reference split node or leaf range, with
+//                     its tight bounding box and the empty-split chain that
+//                     precedes it (kept to prove tree identity);
+//  * TNode[n_tnodes] -- the traversal hierarchy: the reference tree cut at
+//                     nodes of at most `bucket` points, each node holding both
+//                     children's tight boxes, so one 64 B broadcast load per
+//                     warp decides both children.
+//
+// The traversal only needs boxes that contain their points: every result is
+// decided by point distances computed exactly as the reference does, so the
+// tighter boxes change the amount of work, never an answer.
+#pragma once
+
+#include "common.cuh"
+
+namespace pptkg {
+
+template <typename T, int D>
+struct alignas(16) PointRec {
+  T c[D];
+  int32_t id;  // original index of the point
+};
+
+// Build record of one reference node range [begin, end).
+template <typename T, int D>
+struct Rec {
+  T lo[D], hi[D];   // tight bounding box of the range
+  T split_val;      // valid when split_dim >= 0
+  int32_t begin, end;
+  int32_t split_index;
+  int32_t left, right;  // child records, -1 when absent
+  int8_t split_dim;     // -1: leaf range
+  int8_t ntrim;         // empty splits performed before this node (<= 2D)
+  uint8_t trim[2 * D];  // each: dim * 2 + side (0: low side trimmed, 1: high)
+};
+
+// Traversal node: two children, each either an inner node or a leaf bucket.
+template <typename T, int D>
+struct alignas(16) TNode {
+  T lo[2][D], hi[2][D];  // children's tight boxes
+  int32_t ref[2];        // >= 0: TNode index; < 0: leaf, begin = -ref - 1
+  int32_t cnt[2];        // points under the child (0: no child)
+};
+
+template <typename T, int D>
+struct TreeView {
+  const PointRec<T, D>* pts;
+  const TNode<T, D>* nodes;
+  int32_t nv;
+  int32_t depth;    // traversal stack bound (TNode levels)
+  int32_t n_nodes;  // TNode count: no traversal visits more nodes than this
+};
+
+// Host-side owner of one device tree.
+struct TreeBase {
+  int dtype = F32, dim = 3;
+  int64_t n = 0, nv = 0;
+  int n_recs = 0, n_tnodes = 0, depth = 0, tdepth = 0, bucket = 32;
+  int max_leaf = 10;
+  double empty_split = 0.2;
+  int device = 0;
+  void* pts = nullptr;     // PointRec<T, D>[nv]
+  void* recs = nullptr;    // Rec<T, D>[n_recs]
+  void* tnodes = nullptr;  // TNode<T, D>[n_tnodes]
+  int32_t* fwd = nullptr;  // original index -> tree position, -1 if dropped
+  double root_lo[4] = {0, 0, 0, 0}, root_hi[4] = {0, 0, 0, 0};
+  size_t device_bytes() const;
+  ~TreeBase();
+};
+
+}  // namespace pptkg

@@ -1,0 +1,228 @@
+"""GPU parity of the k-d tree build, kNN and r-near (needs a B200).
+
+Everything goes through the public drop-in API, which calls the C ABI.  The
+expected answers come from the reference (golden fixtures) and from the CPU
+oracle, which follows the same (dist2, tree position) tie order as the GPU
+and therefore must agree bit for bit.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from _util import compare_knn, dist2
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = ["f32_uniform", "f64_uniform", "f32_nan_dups", "f32_grid", "f64_aniso"]
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+
+
+def pos_of(rev, n):
+    p = np.full(n, -1, np.int64)
+    p[rev] = np.arange(len(rev))
+    return p
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_build_is_the_reference_tree(gpu, name):
+    g = load(name)
+    t = gpu.kdtree._build(g["points"])
+    assert t.n_valid == len(g["reverse"])
+    assert np.array_equal(t.reverse_indices(), g["reverse"])
+    assert np.array_equal(t.ref_nodes(), g["nodes"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_queries_match_reference(gpu, name):
+    g = load(name)
+    P, Q, k = g["points"], g["queries"], int(g["k"])
+    t = gpu.kdtree._build(P)
+    po = pos_of(g["reverse"], len(P))
+    idx, cnt = gpu.kdtree.knn(t, Q, k)
+    assert compare_knn(idx, cnt, g["knn_idx"], g["knn_cnt"], P, Q, po, k)[0] == 0
+    idx, cnt = gpu.kdtree.knn(t, Q, k, dmax=float(g["knn_r_dmax"]))
+    assert compare_knn(idx, cnt, g["knn_r_idx"], g["knn_r_cnt"], P, Q, po, k)[0] == 0
+    rows = gpu.kdtree._query(t, Q, k=k)
+    assert len(rows) == len(Q) and all(r.dtype == np.int32 for r in rows)
+    assert all(np.array_equal(r, idx_row[:len(r)]) for r, idx_row in zip(rows, gpu.kdtree.knn(t, Q, k)[0]))
+    sq = g["self_q"]
+    sidx, scnt = gpu.kdtree.knn(t, sq, k)
+    assert np.array_equal(scnt, g["self_cnt"])
+    ok = scnt > 0
+    Qs = P[np.where(ok, sq, 0)]
+    assert compare_knn(sidx[ok], scnt[ok], g["self_idx"][ok], g["self_cnt"][ok], P, Qs[ok], po, k)[0] == 0
+    off, out = gpu.kdtree.rnear(t, Q, float(g["rnear_r"]))
+    assert np.array_equal(off, g["rnear_off"]) and np.array_equal(out, g["rnear_idx"])
+    off, out = gpu.kdtree.rnear(t, sq, float(g["rnear_r"]))
+    assert np.array_equal(off, g["rself_off"]) and np.array_equal(out, g["rself_idx"])
+    rows = gpu.kdtree._query(t, sq, k=None, dmax=float(g["rnear_r"]))
+    assert np.array_equal(np.concatenate(rows), g["rself_idx"])
+
+
+@pytest.mark.parametrize("seed,dtype", [(0, np.float32), (1, np.float64)])
+def test_knn_bit_exact_vs_oracle(gpu, port, seed, dtype):
+    # config-1 shape: 200k uniform points, all points as queries, k = 16
+    P = np.random.default_rng(seed).random((200_000, 3)).astype(dtype)
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    assert np.array_equal(t.reverse_indices(), o.reverse_indices())
+    gi, gc = gpu.kdtree.knn(t, None, 16)
+    oi, oc = o.knn_self(np.arange(len(P), dtype=np.int32), 16)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    q = P[::7] + dtype(1e-4)
+    gi, gc = gpu.kdtree.knn(t, q, 16)
+    oi, oc = o.knn(q, 16)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+
+
+def test_bucket_size_never_changes_results(gpu):
+    P = np.random.default_rng(3).random((50_000, 3), dtype=np.float32)
+    t = gpu.kdtree._build(P)
+    base = gpu.kdtree.knn(t, None, 12)
+    r0 = gpu.kdtree.rnear(t, P[:3000], 0.03)
+    for b in (1, 4, 8, 16, 64, 256):
+        t.set_bucket(b)
+        got = gpu.kdtree.knn(t, None, 12)
+        assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1])
+        r = gpu.kdtree.rnear(t, P[:3000], 0.03)
+        assert np.array_equal(r[0], r0[0]) and np.array_equal(r[1], r0[1])
+
+
+def test_rnear_matches_oracle_and_brute_force(gpu, port):
+    rng = np.random.default_rng(4)
+    P = rng.random((30_000, 3), dtype=np.float32)
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    q = rng.random((5000, 3), dtype=np.float32)
+    r = float(np.float32(0.04))
+    off, out = gpu.kdtree.rnear(t, q, r)
+    ooff, oout = o.rnear(q, r)
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+    # brute force on a few rows: hits are exactly the points with dist2 < r^2
+    r2 = np.float32(r) * np.float32(r)
+    for i in range(0, 5000, 997):
+        d = dist2(P, q[i:i + 1], np.arange(len(P))[None, :])[0]
+        assert set(out[off[i]:off[i + 1]].tolist()) == set(np.flatnonzero(d < r2).tolist())
+    # self form drops the query point
+    sidx = np.arange(0, 30_000, 11, dtype=np.int32)
+    off, out = gpu.kdtree.rnear(t, sidx, r)
+    ooff, oout = o.rnear_self(sidx, r)
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+
+
+def test_edge_cases(gpu, port):
+    kd = gpu.kdtree
+    # empty input
+    t = kd._build(np.zeros((0, 3), np.float32))
+    assert t.n_valid == 0
+    idx, cnt = kd.knn(t, np.zeros((4, 3), np.float32), 3)
+    assert (cnt == 0).all() and (idx == -1).all()
+    assert kd._query(t, None, k=2) == []
+    # a single point, fewer points than k, k larger than a leaf
+    P = np.array([[0.5, 0.5, 0.5]], np.float32)
+    t = kd._build(P)
+    assert [r.tolist() for r in kd._query(t, np.array([[0, 0, 0]], np.float32), k=5)] == [[0]]
+    assert [r.tolist() for r in kd._query(t, None, k=5)] == [[]]
+    P = np.random.default_rng(8).random((37, 3), dtype=np.float32)
+    t = kd._build(P)
+    o = port.PortTree(P)
+    gi, gc = kd.knn(t, None, 50)
+    oi, oc = o.knn_self(np.arange(37, dtype=np.int32), 50)
+    assert np.array_equal(gi, oi) and np.array_equal(gc, oc) and (gc == 36).all()
+    # all points identical: one leaf of every point, ties everywhere
+    P = np.ones((500, 3), np.float64)
+    t = kd._build(P)
+    gi, gc = kd.knn(t, None, 7)
+    oi, oc = port.PortTree(P).knn_self(np.arange(500, dtype=np.int32), 7)
+    assert np.array_equal(gi, oi) and np.array_equal(gc, oc)
+    # dmax = 0 finds nothing; NaN rows are dropped and answer nothing
+    P = np.random.default_rng(9).random((1000, 3), dtype=np.float32)
+    P[::10] = np.nan
+    t = kd._build(P)
+    assert t.n_valid == 900
+    idx, cnt = kd.knn(t, P[1:50], 4, dmax=0.0)
+    assert (cnt == 0).all()
+    idx, cnt = kd.knn(t, np.arange(0, 100, dtype=np.int32), 4)
+    assert (cnt[::10] == 0).all() and (cnt[1::10] == 4).all()
+    gi, gc = kd.knn(t, None, 5)  # rows 0 .. num_points()-1, as the reference
+    assert gi.shape == (900, 5)
+    oi, oc = port.PortTree(P).knn_self(np.arange(900, dtype=np.int32), 5)
+    assert np.array_equal(gi, oi) and np.array_equal(gc, oc)
+
+
+def test_query_argument_errors(gpu):
+    kd = gpu.kdtree
+    P = np.random.default_rng(10).random((100, 3))
+    t = kd._build(P)
+    with pytest.raises(ValueError):
+        kd._query(t, np.zeros((0, 2)), k=1)  # wrong dim
+    with pytest.raises(ValueError):
+        kd._query(t, np.zeros((0, 3)), k="a")
+    with pytest.raises(ValueError):
+        kd._query(t, np.zeros((0, 3)), dmax="a")
+    with pytest.raises(ValueError):
+        kd._query(t, P[:2], k=0)
+    with pytest.raises(ValueError):
+        kd._query(t, P[:2], dmax=-1.0)
+    with pytest.raises(ValueError):
+        kd._query(t, P[:2], k=None)  # k=None needs a finite dmax
+    with pytest.raises(RuntimeError):
+        kd._query(t, [0, 100], k=1)
+    with pytest.raises(ValueError):
+        kd._query(t, np.zeros(7, bool), k=1)
+    with pytest.raises(NotImplementedError):
+        kd._query(t, slice(0, 3), k=1)
+    with pytest.raises(TypeError):
+        kd._query("not a tree", P[:2], k=1)
+    with pytest.raises(TypeError):
+        kd._query(t, "abc", k=1)
+    # negative indices wrap; masks select
+    a = kd._query(t, [-1, 0], k=3)
+    b = kd._query(t, [99, 0], k=3)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    m = np.zeros(100, bool)
+    m[[5, 7]] = True
+    c = kd._query(t, m, k=3)
+    d = kd._query(t, [5, 7], k=3)
+    assert all(np.array_equal(x, y) for x, y in zip(c, d))
+    # dmax is rounded through float32, as the reference does
+    r = 0.1 + 1e-12
+    e = kd._query(t, P[:5], k=None, dmax=r)
+    f = kd._query(t, P[:5], k=None, dmax=float(np.float32(r)))
+    assert all(np.array_equal(x, y) for x, y in zip(e, f))
+
+
+def test_torch_cuda_inputs_stay_on_device(gpu):
+    import torch
+    P = torch.rand(20_000, 3, device="cuda")
+    t = gpu.kdtree._build(P)
+    idx, cnt = gpu.kdtree.knn(t, P[:1000], 8)
+    assert idx.is_cuda and idx.shape == (1000, 8)
+    ref_idx, _ = gpu.kdtree.knn(gpu.kdtree._build(P.cpu().numpy()), P[:1000].cpu().numpy(), 8)
+    assert np.array_equal(idx.cpu().numpy(), ref_idx)
+
+
+def test_scene_properties_at_scale(gpu, port):
+    # 2M-point lidar-like scene: full-size properties plus sampled exact rows
+    from pptk_b200 import synth
+    P = synth.lidar_scene(2_000_000, seed=2)
+    t = gpu.kdtree._build(P)
+    idx, cnt = gpu.kdtree.knn(t, None, 32)
+    assert (cnt == 32).all()
+    rows = np.arange(len(P))
+    assert not (idx == rows[:, None]).any()  # self excluded
+    d = dist2(P, P[:200_000], idx[:200_000])
+    assert (np.diff(d, axis=1) >= 0).all()  # ascending distance
+    o = port.PortTree(P)
+    assert np.array_equal(t.reverse_indices(), o.reverse_indices())
+    sample = np.random.default_rng(0).choice(len(P), 20_000, replace=False).astype(np.int32)
+    oi, oc = o.knn_self(sample, 32)
+    assert np.array_equal(idx[sample], oi)
+    off, out = gpu.kdtree.rnear(t, sample, 0.5)
+    ooff, oout = o.rnear_self(sample, 0.5)
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
