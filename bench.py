@@ -228,6 +228,10 @@ def run_ours(args):
 
     norm_ms, norm_cnt = stage("normals")
     build_ms, build_cnt = stage("build")
+    stages = {}
+    for nm in ("build", "build.levels", "build.subtree", "order", "normals"):
+        t_, c_ = stage(nm)
+        stages[nm] = t_ / max(c_, 1) if c_ else 0.0
     lib.pptkg_profile_enable(0)
     ms_t = torch.tensor([ms], device="cuda")
     if world > 1:
@@ -279,7 +283,7 @@ def run_ours(args):
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e,
                 "gpu_launches": int(launches),
-                "stages_ms": {"build": build_ms / max(build_cnt, 1), "normals": norm_launch_ms},
+                "stages_ms": stages,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None,
                              "kernel": "k_normals (fused kNN+PCA)", "peak_kind": peak_kind},

@@ -25,6 +25,7 @@ thread_local int g_code = 0;
 template <typename F>
 int guarded(F&& f) {
   try {
+    keep_pool_cached(0);
     f();
     return PPTKG_OK;
   } catch (const Error& e) {

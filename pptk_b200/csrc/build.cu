@@ -779,7 +779,9 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
   if (n > (int64_t)INT32_MAX - 1) throw Error(E_INVALID, "k-d tree supports at most 2^31-2 points");
   if (max_leaf < 1) max_leaf = 1;
   Stage stage("build", st);
+  keep_pool_cached(st);
   std::unique_ptr<TreeBase> tree(new TreeBase());
+  tree->stream = st;
   tree->dtype = sizeof(T) == 4 ? F32 : F64;
   tree->dim = D;
   tree->n = n;
@@ -847,6 +849,7 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
   int depth = 0;
   if (nv > 0) {
     if (nv > small_cap) {
+      Stage st_levels("build.levels", st);
       DevBuf<Seg<T, D>> segA(1, st), segB;
       PPTKG_CUDA(cudaMemcpyAsync(segA.get(), &root, sizeof(root), cudaMemcpyHostToDevice, st));
       int nA = 1;
@@ -919,6 +922,7 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
       nSmall = 1;
     }
     if (nSmall > 0) {
+      Stage st_sub("build.subtree", st);
       PPTKG_CUDA(cudaFuncSetAttribute(k_subtree<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_subtree<T, D><<<nSmall, SUB_THREADS, smem, st>>>(smallL.get(), soa, recs, small_cap, cap_list, (long long)n,
                                                          max_leaf, thr, (int)rec_cap, ctl.get());
@@ -932,7 +936,7 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
     depth = std::max(depth, hctl.depth);
   }
   tree->depth = depth;
-  PPTKG_CUDA(cudaMalloc(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>)));
+  PPTKG_CUDA(cudaMallocAsync(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>), st));
   if (tree->n_recs)
     PPTKG_CUDA(cudaMemcpyAsync(tree->recs, recs, tree->n_recs * sizeof(Rec<T, D>), cudaMemcpyDeviceToDevice, st));
   recs = (Rec<T, D>*)tree->recs;
@@ -940,9 +944,9 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
 
   // tree-ordered points and the forward map
   PointRec<T, D>* pts = nullptr;
-  PPTKG_CUDA(cudaMalloc(&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>)));
+  PPTKG_CUDA(cudaMallocAsync((void**)&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>), st));
   tree->pts = pts;
-  PPTKG_CUDA(cudaMalloc(&tree->fwd, std::max<int64_t>(n, 1) * sizeof(int)));
+  PPTKG_CUDA(cudaMallocAsync((void**)&tree->fwd, std::max<int64_t>(n, 1) * sizeof(int), st));
   if (n > 0) PPTKG_CUDA(cudaMemsetAsync(tree->fwd, 0xff, n * sizeof(int), st));
   if (nv > 0) {
     k_finish<T, D><<<div_up(nv, 256), 256, 0, st>>>(soa, nv, pts, tree->fwd);
@@ -969,7 +973,7 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
 template <typename T, int D>
 void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
   if (tree->tnodes) {
-    PPTKG_CUDA(cudaFree(tree->tnodes));
+    PPTKG_CUDA(cudaFreeAsync(tree->tnodes, st));
     tree->tnodes = nullptr;
   }
   if (bucket < 1) bucket = 1;
@@ -986,7 +990,7 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
     PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   TNode<T, D>* nodes = nullptr;
-  PPTKG_CUDA(cudaMalloc(&nodes, std::max(nt, 1) * sizeof(TNode<T, D>)));
+  PPTKG_CUDA(cudaMallocAsync((void**)&nodes, std::max(nt, 1) * sizeof(TNode<T, D>), st));
   tree->tnodes = nodes;
   tree->n_tnodes = std::max(nt, 1);
   if (nt > 0) {
@@ -1006,10 +1010,11 @@ size_t TreeBase::device_bytes() const {
 }
 
 TreeBase::~TreeBase() {
-  if (pts) cudaFree(pts);
-  if (recs) cudaFree(recs);
-  if (tnodes) cudaFree(tnodes);
-  if (fwd) cudaFree(fwd);
+  // stream-ordered release on the stream the tree was built on
+  if (pts) cudaFreeAsync(pts, stream);
+  if (recs) cudaFreeAsync(recs, stream);
+  if (tnodes) cudaFreeAsync(tnodes, stream);
+  if (fwd) cudaFreeAsync(fwd, stream);
 }
 
 #define PPTKG_INST_BUILD(T, D)                                                                         \

@@ -154,18 +154,31 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
   bool ok = true;
   int visits = 0;
   auto need = [&](DistT md) { return active && md < r2 && md <= top.worst(); };
+  // Leaf bucket scan in two steps: every lane first marks the candidates that
+  // can enter its list (distance at most its current k-th), with no
+  // divergent branch, then inserts only those.  The warp pays for insertions
+  // once per bucket (the largest count over lanes) rather than once per
+  // candidate that some lane accepts.
   auto scan = [&](int begin, int count) {
     for (int base = begin; base < begin + count; base += 32) {
       const int nb = min(32, begin + count - base);
       __syncwarp();
       if (lane < nb) ws.buf[lane] = tv.pts[base + lane];
       __syncwarp();
+      unsigned mark = 0;
       if (active) {
+        const DistT thr = top.worst();
         for (int t = 0; t < nb; t++) {
-          const PointRec<T, D> pr = ws.buf[t];
-          const DistT d2 = point_dist2<T, DistT, D>(pr.c, q);
-          if (d2 < r2 && base + t != own) top.offer(d2, base + t);
+          const DistT d2 = point_dist2<T, DistT, D>(ws.buf[t].c, q);
+          const bool take = d2 < r2 && d2 <= thr && base + t != own;
+          mark |= (unsigned)take << t;
         }
+      }
+      while (mark) {
+        const int t = __ffs(mark) - 1;
+        mark &= mark - 1;
+        const DistT d2 = point_dist2<T, DistT, D>(ws.buf[t].c, q);
+        top.offer(d2, base + t);
       }
     }
   };
@@ -257,13 +270,20 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
       }
     }
   };
+  // A lane that counted a whole inner child is muted while the warp walks
+  // that child's subtree for other lanes: `mute` is the stack depth at which
+  // the subtree was entered, and the lane rejoins once a pop goes below it.
+  int mute = -1;
+  auto live = [&]() { return active && mute < 0; };
   // Handles child c of nd; returns the node to descend into, or -1.
-  auto process = [&](const TNode<T, D>& nd, int c) -> int {
+  auto process = [&](const TNode<T, D>& nd, int c, bool& took) -> int {
+    took = false;
     if (nd.cnt[c] == 0) return -1;
-    bool mine = active && box_min_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2;
+    bool mine = live() && box_min_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2;
     if (COUNT && mine && box_max_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2) {
       count += nd.cnt[c];
       mine = false;
+      took = true;
     }
     if (!__any_sync(FULL, mine)) return -1;
     const int ref = nd.ref[c];
@@ -280,12 +300,13 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
       break;
     }
     const TNode<T, D>& nd = tv.nodes[cur];
-    const bool w0 = active && nd.cnt[0] > 0 && box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], q) < r2;
-    const bool w1 = active && nd.cnt[1] > 0 && box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) < r2;
+    const bool w0 = live() && nd.cnt[0] > 0 && box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], q) < r2;
+    const bool w1 = live() && nd.cnt[1] > 0 && box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) < r2;
     const bool a0 = __any_sync(FULL, w0), a1 = __any_sync(FULL, w1);
     int next = -1;
+    bool took = false;
     if (a0) {
-      next = process(nd, 0);
+      next = process(nd, 0, took);
       if (next >= 0 && a1) {
         if (sp >= tv.depth) {
           ok = false;
@@ -296,8 +317,9 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
         }
       }
     }
-    if (next < 0 && a1) next = process(nd, 1);
+    if (next < 0 && a1) next = process(nd, 1, took);
     if (next >= 0) {
+      if (took) mute = sp;
       cur = next;
       continue;
     }
@@ -306,8 +328,10 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
     while (sp > 0) {
       const int e = ws.stack[--sp];
       __syncwarp();
-      const int r = process(tv.nodes[e >> 1], e & 1);
+      if (mute >= 0 && sp < mute) mute = -1;
+      const int r = process(tv.nodes[e >> 1], e & 1, took);
       if (r >= 0) {
+        if (took) mute = sp;
         cur = r;
         found = true;
         break;

@@ -56,31 +56,52 @@ __device__ void eigh3(Sym3<P> A, P w[3], P V[9]) {
     // (1, 2): remaining row 0
     jacobi_rotate(A.a11, A.a22, A.a12, A.a01, A.a02, V, 1, 2);
   }
-  P d[3] = {A.a00, A.a11, A.a22};
-  int o0 = 0, o1 = 1, o2 = 2;
-  // stable sort of three values
-  if (d[o1] < d[o0]) { int t = o0; o0 = o1; o1 = t; }
-  if (d[o2] < d[o1]) { int t = o1; o1 = o2; o2 = t; }
-  if (d[o1] < d[o0]) { int t = o0; o0 = o1; o1 = t; }
-  const int ord[3] = {o0, o1, o2};
-  P Vs[9];
+  // order the eigenpairs ascending with compare-exchanges on whole columns
+  // (static register indices only)
+  P d0 = A.a00, d1 = A.a11, d2 = A.a22;
+  P c0[3] = {V[0], V[3], V[6]}, c1[3] = {V[1], V[4], V[7]}, c2[3] = {V[2], V[5], V[8]};
+  auto cx = [](P& da, P* ca, P& db, P* cb) {
+    if (db < da) {
+      P t = da;
+      da = db;
+      db = t;
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const int src = ord[c];
-    w[c] = src == 0 ? d[0] : (src == 1 ? d[1] : d[2]);
-    P v0 = V[0 * 3 + src], v1 = V[1 * 3 + src], v2 = V[2 * 3 + src];
-    int best = 0;
-    P bm = fabs(v0);
-    if (fabs(v1) > bm) { best = 1; bm = fabs(v1); }
-    if (fabs(v2) > bm) { best = 2; }
-    const P sel = best == 0 ? v0 : (best == 1 ? v1 : v2);
-    const P sg = sel < (P)0 ? (P)-1 : (P)1;
-    Vs[0 * 3 + c] = sg * v0;
-    Vs[1 * 3 + c] = sg * v1;
-    Vs[2 * 3 + c] = sg * v2;
+      for (int r = 0; r < 3; r++) {
+        t = ca[r];
+        ca[r] = cb[r];
+        cb[r] = t;
+      }
+    }
+  };
+  cx(d0, c0, d1, c1);
+  cx(d1, c1, d2, c2);
+  cx(d0, c0, d1, c1);
+  auto canon = [](P* c) {
+    // largest-magnitude component positive (first on ties)
+    P sel = c[0], bm = fabs(c[0]);
+    if (fabs(c[1]) > bm) {
+      sel = c[1];
+      bm = fabs(c[1]);
+    }
+    if (fabs(c[2]) > bm) sel = c[2];
+    if (sel < (P)0) {
+      c[0] = -c[0];
+      c[1] = -c[1];
+      c[2] = -c[2];
+    }
+  };
+  canon(c0);
+  canon(c1);
+  canon(c2);
+  w[0] = d0;
+  w[1] = d1;
+  w[2] = d2;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    V[r * 3 + 0] = c0[r];
+    V[r * 3 + 1] = c1[r];
+    V[r * 3 + 2] = c2[r];
   }
-#pragma unroll
-  for (int i = 0; i < 9; i++) V[i] = Vs[i];
 }
 
 // Neumaier compensated accumulator.

@@ -37,6 +37,20 @@ void drain_locked() {
 }
 }  // namespace
 
+void keep_pool_cached(cudaStream_t) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  static std::atomic<unsigned long long> done{0};
+  const unsigned long long bit = 1ull << dev;
+  if (done.load() & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done.fetch_or(bit);
+}
+
 bool profiling_on() {
   std::lock_guard<std::mutex> g(g_mu);
   return g_on;

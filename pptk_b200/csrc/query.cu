@@ -495,11 +495,23 @@ __device__ __forceinline__ void write_invalid(int row, int num_eigen, T* evecs, 
   if (sizes) sizes[row] = 0;
 }
 
+// Blocks per SM that the register budget of a normals kernel aims for: the
+// top-k list takes 2 (float) or 3 (double) registers per slot.
+constexpr int normals_min_blocks(int kmax, int dist_bytes, int prec) {
+  const int need = kmax * (dist_bytes == 4 ? 2 : 3) + (prec == PREC_FP32 ? 32 : 72);
+  const int b = 65536 / (QTHREADS * need);
+  return b < 1 ? 1 : (b > 8 ? 8 : b);
+}
+
+// Fused kNN + PCA.  In the FP32 precision mode a neighbourhood whose two
+// smallest eigenvalues nearly coincide (relative gap < gap_thr) is queued in
+// `fix` for an FP64 re-solve by a second launch of this kernel in FP64 mode.
 template <typename T, int KMAX, typename L, int PREC>
-__global__ void __launch_bounds__(QTHREADS) k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
+__global__ void __launch_bounds__(QTHREADS, normals_min_blocks(KMAX, sizeof(typename DistOf<T>::type), PREC))
+k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
-                                                      int* status) {
+                                                      int* fix, int* nfix, int* status) {
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
@@ -530,16 +542,17 @@ __global__ void __launch_bounds__(QTHREADS) k_normals(TreeView<T, 3> tv, L ld, c
     Sym3<float> C = knn_covariance<T, float, KMAX, DistT>(tv, top, k, q, n);
     float w[3], V[9];
     eigh3<float>(C, w, V);
-    if (!(rel_gap<float>(w) >= (float)gap_thr)) {
-      // small eigen-gap: the normal direction is ill-conditioned in FP32;
-      // redo this neighbourhood in FP64
-      Sym3<double> Cd = knn_covariance<T, double, KMAX, DistT>(tv, top, k, q, n);
-      double wd[3], Vd[9];
-      eigh3<double>(Cd, wd, Vd);
-      write_pca<T, double>(qid, n, wd, Vd, num_eigen, evecs, evals, sizes);
-      return;
-    }
     write_pca<T, float>(qid, n, w, V, num_eigen, evecs, evals, sizes);
+    if (fix && !(rel_gap<float>(w) >= (float)gap_thr)) {
+      // queue [query, count, neighbour positions] for the FP64 re-solve
+      int* e = fix + (int64_t)atomicAdd(nfix, 1) * (KMAX + 2);
+      e[0] = qid;
+      e[1] = n;
+      int c = 0;
+#pragma unroll
+      for (int j = KMAX - 1; j >= 0; j--)
+        if (j < k && top.valid(j)) e[2 + c++] = top.pos(j);
+    }
   }
 }
 
@@ -598,32 +611,97 @@ __global__ void __launch_bounds__(QTHREADS) k_normals_rnear(TreeView<T, 3> tv, L
   write_pca<T, double>(qid, (int)n, w, V, num_eigen, evecs, evals, sizes);
 }
 
+// FP64 re-solve of queued neighbourhoods: one thread per entry, a gather of
+// the stored neighbour positions, float64 covariance (shifted to the query
+// point, centred) and eigensolve; overwrites the FP32 results of that row.
+template <typename T, int KMAX>
+__global__ void k_refine64(const PointRec<T, 3>* pts, const int* fwd, const int* fix, const int* nfix, int num_eigen,
+                           T* evecs, T* evals, int32_t* sizes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *nfix) return;
+  const int* e = fix + (int64_t)i * (KMAX + 2);
+  const int qid = e[0], n = e[1];
+  const PointRec<T, 3> qr = pts[fwd[qid]];
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> r = pts[e[2 + j]];
+    s0 += (double)r.c[0] - (double)qr.c[0];
+    s1 += (double)r.c[1] - (double)qr.c[1];
+    s2 += (double)r.c[2] - (double)qr.c[2];
+  }
+  const double inv = 1.0 / (double)n, m0 = s0 * inv, m1 = s1 * inv, m2 = s2 * inv;
+  Sym3<double> C{0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> r = pts[e[2 + j]];
+    const double a = (double)r.c[0] - (double)qr.c[0] - m0, b = (double)r.c[1] - (double)qr.c[1] - m1,
+                 c = (double)r.c[2] - (double)qr.c[2] - m2;
+    C.a00 += a * a;
+    C.a01 += a * b;
+    C.a02 += a * c;
+    C.a11 += b * b;
+    C.a12 += b * c;
+    C.a22 += c * c;
+  }
+  C.a00 *= inv;
+  C.a01 *= inv;
+  C.a02 *= inv;
+  C.a11 *= inv;
+  C.a12 *= inv;
+  C.a22 *= inv;
+  double w[3], V[9];
+  eigh3<double>(C, w, V);
+  write_pca<T, double>(qid, n, w, V, num_eigen, evecs, evals, sizes);
+}
+
 template <typename T, int KMAX, typename L, int PREC>
 void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
-                    int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st) {
+                    int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
+                    cudaStream_t st) {
+  if (m <= 0) return;
   const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth);
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, 3>(t), ld, order, mode, m, k, r2,
-                                                                             num_eigen, gap_thr, ev, ew, sz, status);
+  k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
+      view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status);
   PPTKG_CHECK_LAUNCH();
 }
 
-template <typename T, typename L, int PREC>
+template <typename T, int KMAX, typename L>
+void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                  int num_eigen, int prec, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st) {
+  if (prec == PREC_FP64) {
+    launch_normals<T, KMAX, L, PREC_FP64>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, nullptr,
+                                          nullptr, status, st);
+    return;
+  }
+  // FP32 pass, then an FP64 re-solve of the queued small-gap neighbourhoods
+  DevBuf<int> fix((size_t)std::max(m, 1) * (KMAX + 2), st), nfix(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(nfix.get(), 0, sizeof(int), st));
+  launch_normals<T, KMAX, L, PREC_FP32>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix.get(),
+                                        nfix.get(), status, st);
+  {
+    Stage s("normals.refine64", st);
+    k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, t->fwd, fix.get(), nfix.get(),
+                                                        num_eigen, ev, ew, sz);
+    PPTKG_CHECK_LAUNCH();
+  }
+}
+
+template <typename T, typename L>
 void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k,
-                      typename DistOf<T>::type r2, int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz,
-                      int* status, cudaStream_t st) {
+                      typename DistOf<T>::type r2, int num_eigen, int prec, double gap_thr, T* ev, T* ew,
+                      int32_t* sz, int* status, cudaStream_t st) {
   if (k <= 4)
-    launch_normals<T, 4, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
   else if (k <= 8)
-    launch_normals<T, 8, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
   else if (k <= 16)
-    launch_normals<T, 16, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
   else if (k <= 32)
-    launch_normals<T, 32, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
   else
-    launch_normals<T, 64, L, PREC>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
 }
 
 template <typename T>
@@ -662,12 +740,8 @@ void normals_query(const TreeBase* t, const QuerySpec& qs_in, int k, float r, in
   } else {
     int prec = precision;
     if (prec == PREC_AUTO) prec = sizeof(T) == 4 ? PREC_FP32 : PREC_FP64;
-    if (prec == PREC_FP64)
-      dispatch_normals<T, IndexQueries<3, false>, PREC_FP64>(t, ld, order.get(), mode, m, k, r2, num_eigen, gap_thr,
-                                                             d_evecs, d_evals, d_sizes, status.get(), st);
-    else
-      dispatch_normals<T, IndexQueries<3, false>, PREC_FP32>(t, ld, order.get(), mode, m, k, r2, num_eigen, gap_thr,
-                                                             d_evecs, d_evals, d_sizes, status.get(), st);
+    dispatch_normals<T, IndexQueries<3, false>>(t, ld, order.get(), mode, m, k, r2, num_eigen, prec, gap_thr, d_evecs,
+                                                d_evals, d_sizes, status.get(), st);
   }
   check_status(status.get(), st, "normals");
 }

@@ -68,6 +68,7 @@ struct TreeBase {
   int max_leaf = 10;
   double empty_split = 0.2;
   int device = 0;
+  cudaStream_t stream = 0;  // allocations are stream-ordered on this stream
   void* pts = nullptr;     // PointRec<T, D>[nv]
   void* recs = nullptr;    // Rec<T, D>[n_recs]
   void* tnodes = nullptr;  // TNode<T, D>[n_tnodes]

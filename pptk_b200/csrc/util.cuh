@@ -6,6 +6,11 @@
 
 namespace pptkg {
 
+// Keeps freed blocks of the device's default memory pool cached instead of
+// returning them to the driver at every synchronisation (the default release
+// threshold is 0), so repeated calls reuse their scratch without remapping.
+void keep_pool_cached(cudaStream_t st);
+
 // ------------------------------------------------------------- DevBuf ----
 // Scratch memory from the device's stream-ordered pool (cudaMallocAsync); it
 // is returned to the pool on the same stream when the buffer goes away.
