@@ -146,6 +146,26 @@ PPTKG_API int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices,
                        int num_eigen, int precision, void* out_evecs, void* out_evals, int32_t* out_sizes,
                        void* stream);
 
+/* Allocation-free form of pptkg_tree_normals.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory, such as
+ * code running under another framework that has reserved the GPU's memory up
+ * front, or latency-critical loops where a cudaMalloc (which can synchronize
+ * the device) is not acceptable.  The caller passes device pointers for the
+ * query rows (indices, or NULL for rows 0..m-1; m = 0 with NULL means all
+ * rows) and for the outputs, as in pptkg_tree_normals with PPTKG_MEM_DEVICE.
+ * Limits: m <= PPTKG_NOALLOC_MAX_QUERIES (65536), 1 <= k <= 16; larger sizes
+ * are rejected with PPTKG_E_INVALID.  The scratch (about 4.7 MB) is a static
+ * device array held by every GPU that loads the library until the process
+ * exits; the first call on a device looks up its address, so make that first
+ * call before any stream capture.  All calls share that one array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialized by the caller.  No memory is allocated or freed. */
+#define PPTKG_NOALLOC_MAX_QUERIES 65536
+#define PPTKG_NOALLOC_MAX_K 16
+PPTKG_API int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* indices, int64_t m, int k, float r,
+                                         int num_eigen, int precision, void* out_evecs, void* out_evals,
+                                         int32_t* out_sizes, void* stream);
+
 /* Batched symmetric 3x3 eigensolve of m row-major matrices of dtype F32/F64:
  * w m x 3 ascending; V m x 3 x 3 with layout 0: V[i, :, j] = j-th
  * eigenvector (vfuncs._eigh, pptk/vfuncs/vfuncs.cpp:1241-1293), layout 1:

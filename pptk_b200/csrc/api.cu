@@ -467,6 +467,26 @@ int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices, int64_t m
   });
 }
 
+int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* indices, int64_t m, int k, float r,
+                               int num_eigen, int precision, void* out_evecs, void* out_evals, int32_t* out_sizes,
+                               void* stream) {
+  return guarded([&] {
+    const TreeBase* t = tree_of(tree);
+    DeviceGuard g(t->device);
+    if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+    if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
+    if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
+    if (precision < PPTKG_PREC_AUTO || precision > PPTKG_PREC_FP64) throw Error(E_INVALID, "unknown precision");
+    if (!indices && m == 0) m = t->n;
+    if (m > 0 && !out_evecs && !out_evals && !out_sizes) throw Error(E_INVALID, "no output requested");
+    dispatch_float(t->dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      normals_noalloc<T>(t, indices, m, k, r, num_eigen, precision, (T*)out_evecs, (T*)out_evals, out_sizes,
+                         S(stream));
+    });
+  });
+}
+
 int pptkg_eigh3(const void* A, int64_t m, int dtype, int mem, void* w, void* V, int layout, void* stream) {
   return guarded([&] {
     if (m < 0) throw Error(E_INVALID, "negative count");

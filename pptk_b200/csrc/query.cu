@@ -1,6 +1,8 @@
 // Query kernels: exact kNN (point and self forms), r-near count/fill in the
 // reference's order, and fused kNN + PCA normal estimation.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "knn.cuh"
 #include "normals.cuh"
@@ -774,6 +776,101 @@ void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStre
   k_eigh3<T><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(d_A, m, d_w, d_V, layout);
   PPTKG_CHECK_LAUNCH();
 }
+
+// ------------------------------------------- allocation-free normals ----
+// Scratch of pptkg_tree_normals_noalloc, resident on every GPU that loads the
+// library: [0] status word, [1] FP64 re-solve queue length, then (from int 64,
+// 256-byte aligned) the queue itself, NOALLOC_MAX_QUERIES entries of up to
+// NOALLOC_MAX_K + 2 ints.  About 4.7 MB.
+constexpr int NOALLOC_MAX_QUERIES = 65536;
+constexpr int NOALLOC_MAX_K = 16;
+constexpr int NOALLOC_QUEUE_OFFSET = 64;
+static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_QUEUE_OFFSET +
+                                                       NOALLOC_MAX_QUERIES * (NOALLOC_MAX_K + 2)];
+
+// Device address of the scratch array on the current device.  Host code
+// cannot use the symbol itself (it names a host-side stand-in), so the
+// address is looked up once per device with that device current.
+static int* noalloc_scratch() {
+  static std::mutex mu;
+  static int* addr[64] = {};
+  int dev = 0;
+  PPTKG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(E_CUDA, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[dev]) {
+    int* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw Error(E_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
+template <typename T, int KMAX>
+static void normals_noalloc_k(const TreeBase* t, const int32_t* idx, int m, int k, typename DistOf<T>::type r2,
+                              int num_eigen, int prec, T* ev, T* ew, int32_t* sz, int* scratch, cudaStream_t st) {
+  typedef IndexQueries<3, false> L;
+  L ld{idx, t->fwd};
+  const int mode = (!idx && m == t->nv && t->n == t->nv) ? 2 : 0;
+  int* status = scratch;
+  int* nfix = scratch + 1;
+  int* fix = scratch + NOALLOC_QUEUE_OFFSET;
+  if (prec == PREC_FP64) {
+    launch_normals<T, KMAX, L, PREC_FP64>(t, ld, nullptr, mode, m, k, r2, num_eigen, 0.0, ev, ew, sz, nullptr,
+                                          nullptr, status, st);
+    return;
+  }
+  launch_normals<T, KMAX, L, PREC_FP32>(t, ld, nullptr, mode, m, k, r2, num_eigen, 1e-3, ev, ew, sz, fix, nfix,
+                                        status, st);
+  k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, t->fwd, fix, nfix, num_eigen,
+                                                      ev, ew, sz);
+  PPTKG_CHECK_LAUNCH();
+}
+
+template <typename T>
+void normals_noalloc(const TreeBase* t, const int32_t* d_idx, int64_t m, int k, float r, int num_eigen, int precision,
+                     T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k < 1 || k > NOALLOC_MAX_K)
+    throw Error(E_INVALID, "k must be in [1, " + std::to_string(NOALLOC_MAX_K) + "] for the allocation-free entry");
+  if (m < 0 || m > NOALLOC_MAX_QUERIES)
+    throw Error(E_INVALID, "query count " + std::to_string(m) + " exceeds the allocation-free limit of " +
+                               std::to_string(NOALLOC_MAX_QUERIES));
+  if (!d_idx && m > t->n) throw Error(E_RANGE, "query rows exceed the point count");
+  int* scratch = noalloc_scratch();
+  if (m == 0) return;
+  // status and queue length start at zero; the queue itself needs no clearing
+  PPTKG_CUDA(cudaMemsetAsync(scratch, 0, 2 * sizeof(int), st));
+  int h = 0;
+  if (d_idx) {
+    k_check_idx<<<div_up(m, 256), 256, 0, st>>>(d_idx, (int)m, (int)t->n, scratch);
+    PPTKG_CHECK_LAUNCH();
+    PPTKG_CUDA(cudaMemcpyAsync(&h, scratch, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+    if (h) throw Error(E_RANGE, "query index outside of [0, n)");
+  }
+  const DistT rr = (DistT)(T)r;
+  const DistT r2 = rr * rr;
+  int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
+  const int mi = (int)m;
+  if (k <= 4)
+    normals_noalloc_k<T, 4>(t, d_idx, mi, k, r2, num_eigen, prec, d_evecs, d_evals, d_sizes, scratch, st);
+  else if (k <= 8)
+    normals_noalloc_k<T, 8>(t, d_idx, mi, k, r2, num_eigen, prec, d_evecs, d_evals, d_sizes, scratch, st);
+  else
+    normals_noalloc_k<T, 16>(t, d_idx, mi, k, r2, num_eigen, prec, d_evecs, d_evals, d_sizes, scratch, st);
+  PPTKG_CUDA(cudaMemcpyAsync(&h, scratch, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h) throw Error(E_DEVICE, "normals (allocation-free): device traversal check failed (code " +
+                                   std::to_string(h) + ")");
+}
+
+template void normals_noalloc<float>(const TreeBase*, const int32_t*, int64_t, int, float, int, int, float*, float*,
+                                     int32_t*, cudaStream_t);
+template void normals_noalloc<double>(const TreeBase*, const int32_t*, int64_t, int, float, int, int, double*,
+                                      double*, int32_t*, cudaStream_t);
 
 #define PPTKG_INST_Q(T, D)                                                                                 \
   template void knn_query<T, D>(const TreeBase*, const QuerySpec&, int, double, int32_t*, int32_t*,        \

@@ -41,6 +41,12 @@ template <typename T>
 void normals_query(const TreeBase* t, const QuerySpec& qs, int k, float r, int num_eigen, int precision,
                    double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st);
 
+// pptkg_tree_normals_noalloc: the tree-normals path with its scratch in a
+// static device array instead of allocated memory (device pointers only).
+template <typename T>
+void normals_noalloc(const TreeBase* t, const int32_t* d_idx, int64_t m, int k, float r, int num_eigen, int precision,
+                     T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st);
+
 // Batched symmetric 3x3 eigensolve (row-major inputs).
 template <typename T>
 void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStream_t st);
