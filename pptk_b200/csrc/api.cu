@@ -129,7 +129,7 @@ struct DeviceGuard {
   }
 };
 
-constexpr int DEFAULT_BUCKET = 32;
+constexpr int DEFAULT_BUCKET = 64;
 constexpr double DEFAULT_GAP = 1e-3;
 
 // Preorder serialization of the reference node list (node.h:15-29): each

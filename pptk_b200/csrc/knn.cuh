@@ -89,6 +89,7 @@ struct TopK<KMAX, float> {
     }
     s[KMAX - 1] = s[KMAX - 1] > c ? c : s[KMAX - 1];
   }
+  __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return s[j] < lim; }
   __device__ __forceinline__ int pos(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
   __device__ __forceinline__ float dist(int j) const { return __uint_as_float((unsigned)(s[j] >> 32)); }
@@ -126,6 +127,7 @@ struct TopK<KMAX, double> {
       p[KMAX - 1] = cp;
     }
   }
+  __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && d[j] >= 0.0; }
   __device__ __forceinline__ int pos(int j) const { return p[j]; }
   __device__ __forceinline__ double dist(int j) const { return d[j]; }
@@ -136,98 +138,178 @@ struct TopK<KMAX, double> {
 template <typename T, int D>
 struct WarpScratch {
   int* stack;
-  PointRec<T, D>* buf;  // 32 entries
+  PointRec<T, D>* buf;                   // 32 entries (r-near staging)
+  int* log;                              // per-lane neighbour lists, lane-strided; null when unused
+  typename DistOf<T>::type* dmat;        // 32 x 33 distances (kNN bucket scan); null when unused
 };
+
+// One deferred child on the per-warp traversal stack: its box travels with
+// it, so a pop re-tests the box from shared memory without touching the node
+// array.  ref >= 0: inner node; ref < 0: leaf bucket starting at -ref - 1.
+template <typename T, int D>
+struct StackEnt {
+  T lo[D], hi[D];
+  int ref, cnt;
+};
+
+template <typename T, int D>
+__device__ __forceinline__ TNode<T, D> load_node(const TNode<T, D>* nodes, int i) {
+  static_assert(sizeof(TNode<T, D>) % 16 == 0, "TNode must be a multiple of 16 bytes");
+  TNode<T, D> n;
+  const float4* src = reinterpret_cast<const float4*>(nodes + i);
+  float4* dst = reinterpret_cast<float4*>(&n);
+#pragma unroll
+  for (int j = 0; j < (int)(sizeof(TNode<T, D>) / 16); j++) dst[j] = __ldg(src + j);
+  return n;
+}
 
 // Exact kNN of the lane's query over the whole tree, ties in dist2 broken by
 // tree position.  `own` (tree position or -1) is skipped, which is how self
 // queries exclude the query point itself.  Returns false when the traversal
 // stack would overflow (the host sizes it from the tree depth, so this is a
 // safety net that reports instead of corrupting memory).
-template <typename T, int D, int KMAX, typename DistT>
-__device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2,
-                           TopK<KMAX, DistT>& top, WarpScratch<T, D> ws) {
+//
+// The walk hides the latency of the dependent node loads: the node to
+// descend into is loaded before the sibling bucket is scanned, and deferred
+// children carry their boxes on the stack.
+template <typename T, int D, typename Top, typename DistT>
+__device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top,
+                           WarpScratch<T, D> ws) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
+  StackEnt<T, D>* stk = reinterpret_cast<StackEnt<T, D>*>(ws.stack);
   int sp = 0;
-  int cur = 0;
   bool ok = true;
   int visits = 0;
   auto need = [&](DistT md) { return active && md < r2 && md <= top.worst(); };
-  // Leaf bucket scan in two steps: every lane first marks the candidates that
-  // can enter its list (distance at most its current k-th), with no
-  // divergent branch, then inserts only those.  The warp pays for insertions
-  // once per bucket (the largest count over lanes) rather than once per
-  // candidate that some lane accepts.
-  auto scan = [&](int begin, int count) {
+  // Leaf bucket scan, transposed: lane j holds candidate j of the chunk
+  // (one coalesced 16 B load), and the warp loops only over the lanes whose
+  // query needs this bucket.  For such a query i every lane computes its
+  // candidate's distance to q_i; the row goes to dmat[i][*] and the ballot of
+  // candidates that can enter list i becomes lane i's mark mask.  Each lane
+  // then inserts its marked candidates, reading distances from its row.
+  auto scan = [&](int begin, int count, bool mine) {
+    const unsigned needm = __ballot_sync(FULL, mine);
     for (int base = begin; base < begin + count; base += 32) {
       const int nb = min(32, begin + count - base);
-      __syncwarp();
-      if (lane < nb) ws.buf[lane] = tv.pts[base + lane];
-      __syncwarp();
-      unsigned mark = 0;
-      if (active) {
-        const DistT thr = top.worst();
-        for (int t = 0; t < nb; t++) {
-          const DistT d2 = point_dist2<T, DistT, D>(ws.buf[t].c, q);
-          const bool take = d2 < r2 && d2 <= thr && base + t != own;
-          mark |= (unsigned)take << t;
-        }
+      PointRec<T, D> pr;
+      if (lane < nb) {
+        pr = tv.pts[base + lane];
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) pr.c[d] = (T)0;
       }
+      const DistT thr_mine = top.worst();
+      unsigned mark = 0;
+      unsigned rem = needm;
+      while (rem) {
+        const int i = __ffs(rem) - 1;
+        rem &= rem - 1;
+        DistT qi[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) qi[d] = __shfl_sync(FULL, q[d], i);
+        const DistT thr = __shfl_sync(FULL, thr_mine, i);
+        const int own_i = __shfl_sync(FULL, own, i);
+        const DistT d2 = point_dist2<T, DistT, D>(pr.c, qi);
+        ws.dmat[i * 33 + lane] = d2;
+        const unsigned m = __ballot_sync(FULL, lane < nb && d2 <= thr && d2 < r2 && base + lane != own_i);
+        if (lane == i) mark = m;
+      }
+      __syncwarp();
+      top.reserve(__popc(mark));
       while (mark) {
         const int t = __ffs(mark) - 1;
         mark &= mark - 1;
-        const DistT d2 = point_dist2<T, DistT, D>(ws.buf[t].c, q);
-        top.offer(d2, base + t);
+        top.offer(ws.dmat[lane * 33 + t], base + t);
       }
+      __syncwarp();
     }
   };
+  auto push = [&](const T* lo, const T* hi, int ref, int cnt) {
+    if (sp >= tv.depth) {
+      ok = false;
+      return;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      StackEnt<T, D> e;
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        e.lo[d] = lo[d];
+        e.hi[d] = hi[d];
+      }
+      e.ref = ref;
+      e.cnt = cnt;
+      stk[sp] = e;
+    }
+    sp++;
+  };
+  TNode<T, D> nd = load_node(tv.nodes, 0);
   while (true) {
     if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
       ok = false;
       break;
     }
-    const TNode<T, D>& nd = tv.nodes[cur];
     DistT md[2];
     md[0] = nd.cnt[0] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], q) : (DistT)INFINITY;
     md[1] = nd.cnt[1] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) : (DistT)INFINITY;
-    const int first = __popc(__ballot_sync(FULL, active && md[1] < md[0])) > __popc(__ballot_sync(FULL, active)) / 2;
+    // near child first, by majority vote; children unpacked with selects
+    // (no run-time register indexing)
+    const bool sw = __popc(__ballot_sync(FULL, active && md[1] < md[0])) > __popc(__ballot_sync(FULL, active)) / 2;
+    const DistT md0 = sw ? md[1] : md[0], md1 = sw ? md[0] : md[1];
+    const int ref0 = sw ? nd.ref[1] : nd.ref[0], ref1 = sw ? nd.ref[0] : nd.ref[1];
+    const int cnt0 = sw ? nd.cnt[1] : nd.cnt[0], cnt1 = sw ? nd.cnt[0] : nd.cnt[1];
+    const bool m0 = need(md0);
+    const bool a0 = __any_sync(FULL, m0);
+    const bool a1 = __any_sync(FULL, need(md1));
     int next = -1;
+    TNode<T, D> nn;
+    if (a0 && ref0 >= 0) {
+      // near child is an inner node: fetch it now, defer the far child
+      next = ref0;
+      nn = load_node(tv.nodes, next);
+      if (a1) {
+        T lo1[D], hi1[D];
 #pragma unroll
-    for (int o = 0; o < 2; o++) {
-      const int c = o == 0 ? first : 1 - first;
-      if (!__any_sync(FULL, need(md[c]))) continue;
-      const int ref = nd.ref[c];
-      if (ref < 0) {
-        scan(-ref - 1, nd.cnt[c]);
-      } else if (next < 0) {
-        next = ref;
-      } else {
-        if (sp >= tv.depth) {
-          ok = false;
-        } else {
-          if (lane == 0) ws.stack[sp] = (cur << 1) | c;
-          sp++;
+        for (int d = 0; d < D; d++) {
+          lo1[d] = sw ? nd.lo[0][d] : nd.lo[1][d];
+          hi1[d] = sw ? nd.hi[0][d] : nd.hi[1][d];
         }
+        push(lo1, hi1, ref1, cnt1);
+      }
+    } else {
+      if (a1 && ref1 >= 0) {
+        // far child is an inner node: its fetch overlaps the near bucket scan
+        next = ref1;
+        nn = load_node(tv.nodes, next);
+      }
+      if (a0) scan(-ref0 - 1, cnt0, m0);
+      const bool m1 = need(md1);  // re-test against the tightened threshold
+      if (!__any_sync(FULL, m1)) {
+        next = -1;
+      } else if (ref1 < 0) {
+        scan(-ref1 - 1, cnt1, m1);
       }
     }
     if (next >= 0) {
-      cur = next;
+      nd = nn;
       continue;
     }
     __syncwarp();
     bool found = false;
     while (sp > 0) {
-      const int e = ws.stack[--sp];
+      --sp;
+      const StackEnt<T, D> e = stk[sp];
       __syncwarp();
-      const TNode<T, D>& pn = tv.nodes[e >> 1];
-      const int c = e & 1;
-      const DistT m = box_min_dist2<T, DistT, D>(pn.lo[c], pn.hi[c], q);
-      if (__any_sync(FULL, need(m))) {
-        cur = pn.ref[c];
-        found = true;
-        break;
+      const bool me = need(box_min_dist2<T, DistT, D>(e.lo, e.hi, q));
+      if (!__any_sync(FULL, me)) continue;
+      if (e.ref < 0) {
+        scan(-e.ref - 1, e.cnt, me);
+        continue;
       }
+      nd = load_node(tv.nodes, e.ref);
+      found = true;
+      break;
     }
     __syncwarp();
     if (!found) break;

@@ -26,21 +26,35 @@ TreeView<T, D> view_of(const TreeBase* t) {
   return v;
 }
 
+// Per-warp shared memory: leaf staging buffer (r-near), traversal stack, the
+// 32 x 33 distance matrix of the kNN bucket scan, and (normals) `logcap`
+// list slots per lane.
 template <typename T, int D>
-size_t warp_smem_bytes(int depth) {
-  return 32 * sizeof(PointRec<T, D>) + (((size_t)depth * 4 + 15) & ~(size_t)15);
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
+  typedef typename DistOf<T>::type DistT;
+  return 32 * sizeof(PointRec<T, D>) + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
+         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + (size_t)logcap * 32 * 4;
 }
 
 template <typename T, int D>
-__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth) {
+__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0) {
+  typedef typename DistOf<T>::type DistT;
   extern __shared__ __align__(16) unsigned char qsm[];
-  const size_t per = 32 * sizeof(PointRec<T, D>) + (((size_t)depth * 4 + 15) & ~(size_t)15);
+  const size_t per = warp_smem_bytes<T, D>(depth, logcap);
   unsigned char* base = qsm + (threadIdx.x >> 5) * per;
   WarpScratch<T, D> ws;
   ws.buf = (PointRec<T, D>*)base;
-  ws.stack = (int*)(base + 32 * sizeof(PointRec<T, D>));
+  base += 32 * sizeof(PointRec<T, D>);
+  ws.stack = (int*)base;
+  base += ((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15;
+  ws.dmat = (DistT*)base;
+  base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
+  ws.log = logcap ? (int*)base : nullptr;
   return ws;
 }
+
+// Candidate-log capacity per lane of the normals kernel.
+__host__ __device__ constexpr int normals_logcap(int kmax) { return 2 * kmax; }
 
 // ------------------------------------------------------------- loaders ----
 // Query i is row i of a user array.
@@ -200,7 +214,7 @@ __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const
     for (int d = 0; d < D; d++) q[d] = (DistT)0;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (!packet_knn<T, D, KMAX, DistT>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (!packet_knn<T, D>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
   if (slot < m) {
     int c = 0;
 #pragma unroll
@@ -418,40 +432,32 @@ void rnear_fill(const TreeBase* t, const QuerySpec& qs, double dmax, const int64
 // ------------------------------------------------------------- normals ----
 // Covariance of the neighbourhood in precision P, each neighbour shifted to
 // the query point first (p - q, formed in the input type's precision or
-// better), then mean-centred in a second pass with compensated sums.
-template <typename T, typename P, int KMAX, typename DistT>
-__device__ __forceinline__ Sym3<P> knn_covariance(const TreeView<T, 3>& tv, const TopK<KMAX, DistT>& top, int k,
-                                                  const DistT* q, int& n) {
+// better), then mean-centred in a second pass with compensated sums.  The
+// neighbours are the tree positions log[i * 32], i < n.
+template <typename T, typename P, typename DistT>
+__device__ __forceinline__ Sym3<P> log_covariance(const TreeView<T, 3>& tv, const int* log, int n, const DistT* q) {
   typedef typename std::conditional<(sizeof(T) > sizeof(P)), T, P>::type W;
   P s0 = 0, s1 = 0, s2 = 0;
-  n = 0;
-#pragma unroll
-  for (int j = 0; j < KMAX; j++) {
-    if (j < k && top.valid(j)) {
-      const PointRec<T, 3> r = tv.pts[top.pos(j)];
-      s0 += (P)((W)r.c[0] - (W)q[0]);
-      s1 += (P)((W)r.c[1] - (W)q[1]);
-      s2 += (P)((W)r.c[2] - (W)q[2]);
-      n++;
-    }
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> r = tv.pts[log[j * 32]];
+    s0 += (P)((W)r.c[0] - (W)q[0]);
+    s1 += (P)((W)r.c[1] - (W)q[1]);
+    s2 += (P)((W)r.c[2] - (W)q[2]);
   }
   const P inv = n > 0 ? (P)1 / (P)n : (P)0;
   const P m0 = s0 * inv, m1 = s1 * inv, m2 = s2 * inv;
   CSum<P> c00, c01, c02, c11, c12, c22;
-#pragma unroll
-  for (int j = 0; j < KMAX; j++) {
-    if (j < k && top.valid(j)) {
-      const PointRec<T, 3> r = tv.pts[top.pos(j)];
-      const P e0 = (P)((W)r.c[0] - (W)q[0]) - m0;
-      const P e1 = (P)((W)r.c[1] - (W)q[1]) - m1;
-      const P e2 = (P)((W)r.c[2] - (W)q[2]) - m2;
-      c00.add(e0 * e0);
-      c01.add(e0 * e1);
-      c02.add(e0 * e2);
-      c11.add(e1 * e1);
-      c12.add(e1 * e2);
-      c22.add(e2 * e2);
-    }
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> r = tv.pts[log[j * 32]];
+    const P e0 = (P)((W)r.c[0] - (W)q[0]) - m0;
+    const P e1 = (P)((W)r.c[1] - (W)q[1]) - m1;
+    const P e2 = (P)((W)r.c[2] - (W)q[2]) - m2;
+    c00.add(e0 * e0);
+    c01.add(e0 * e1);
+    c02.add(e0 * e2);
+    c11.add(e1 * e1);
+    c12.add(e1 * e2);
+    c22.add(e2 * e2);
   }
   Sym3<P> C;
   C.a00 = c00.value() * inv;
@@ -500,7 +506,7 @@ __device__ __forceinline__ void write_invalid(int row, int num_eigen, T* evecs, 
 // Blocks per SM that the register budget of a normals kernel aims for: the
 // top-k list takes 2 (float) or 3 (double) registers per slot.
 constexpr int normals_min_blocks(int kmax, int dist_bytes, int prec) {
-  const int need = kmax * (dist_bytes == 4 ? 2 : 3) + (prec == PREC_FP32 ? 32 : 72);
+  const int need = kmax * (dist_bytes == 4 ? 2 : 3) + (prec == PREC_FP32 ? 64 : 72);
   const int b = 65536 / (QTHREADS * need);
   return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
@@ -515,9 +521,11 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
                                                       int* fix, int* nfix, int* status) {
   typedef typename DistOf<T>::type DistT;
+  constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth);
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
+  const int lane = threadIdx.x & 31;
   int qid = -1, own = -1;
   DistT q[3];
   bool active = false;
@@ -526,22 +534,26 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
     active = ld.load(qid, tv, q, own);
   }
   if (!active) q[0] = q[1] = q[2] = (DistT)0;
+  int* lane_log = ws.log + lane;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (!packet_knn<T, 3, KMAX, DistT>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (!packet_knn<T, 3>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
   if (slot >= m) return;
   if (!active) {
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
     return;
   }
-  int n;
+  int n = 0;
+#pragma unroll
+  for (int j = KMAX - 1; j >= 0; j--)
+    if (j < k && top.valid(j)) lane_log[(n++) * 32] = top.pos(j);
   if (PREC == PREC_FP64) {
-    Sym3<double> C = knn_covariance<T, double, KMAX, DistT>(tv, top, k, q, n);
+    Sym3<double> C = log_covariance<T, double, DistT>(tv, lane_log, n, q);
     double w[3], V[9];
     eigh3<double>(C, w, V);
     write_pca<T, double>(qid, n, w, V, num_eigen, evecs, evals, sizes);
   } else {
-    Sym3<float> C = knn_covariance<T, float, KMAX, DistT>(tv, top, k, q, n);
+    Sym3<float> C = log_covariance<T, float, DistT>(tv, lane_log, n, q);
     float w[3], V[9];
     eigh3<float>(C, w, V);
     write_pca<T, float>(qid, n, w, V, num_eigen, evecs, evals, sizes);
@@ -550,10 +562,7 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
       int* e = fix + (int64_t)atomicAdd(nfix, 1) * (KMAX + 2);
       e[0] = qid;
       e[1] = n;
-      int c = 0;
-#pragma unroll
-      for (int j = KMAX - 1; j >= 0; j--)
-        if (j < k && top.valid(j)) e[2 + c++] = top.pos(j);
+      for (int j = 0; j < n; j++) e[2 + j] = lane_log[j * 32];
     }
   }
 }
@@ -660,7 +669,7 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
                     cudaStream_t st) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth);
+  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
