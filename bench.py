@@ -229,7 +229,8 @@ def run_ours(args):
     norm_ms, norm_cnt = stage("normals")
     build_ms, build_cnt = stage("build")
     stages = {}
-    for nm in ("build", "build.levels", "build.subtree", "order", "normals"):
+    for nm in ("build", "build.prep", "build.attempt", "build.levels", "build.subtree", "build.finish",
+               "build.tnodes", "order", "normals"):
         t_, c_ = stage(nm)
         stages[nm] = t_ / max(c_, 1) if c_ else 0.0
     lib.pptkg_profile_enable(0)

@@ -287,9 +287,10 @@ int pptkg_tree_reverse_indices(const pptkg_tree* tree, int32_t* out, int mem, vo
   });
 }
 
-int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, int64_t* count) {
+static int ref_nodes(const pptkg_tree* tree, int cloud, double* out, int64_t capacity, int64_t* count) {
   return guarded([&] {
     const TreeBase* t = tree_of(tree);
+    if (cloud < -1 || cloud >= t->ncloud) throw Error(E_INVALID, "cloud index out of range");
     DeviceGuard g(t->device);
     dispatch_build(t->dtype, t->dim, [&](auto tt, auto d) {
       typedef decltype(tt) T;
@@ -297,8 +298,10 @@ int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, 
       std::vector<Rec<T, Dm>> recs(t->n_recs);
       if (t->n_recs)
         PPTKG_CUDA(cudaMemcpy(recs.data(), t->recs, sizeof(Rec<T, Dm>) * t->n_recs, cudaMemcpyDeviceToHost));
+      int root = -1;
+      PPTKG_CUDA(cudaMemcpy(&root, t->root_rec + (cloud < 0 ? 0 : cloud), sizeof(int), cudaMemcpyDeviceToHost));
       std::vector<double> v;
-      if (t->n_recs) serialize_nodes<T, Dm>(recs, 0, v);
+      if (t->n_recs && root >= 0) serialize_nodes<T, Dm>(recs, root, v);
       const int64_t cnt = (int64_t)(v.size() / 5);
       if (count) *count = cnt;
       if (out) {
@@ -307,6 +310,10 @@ int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, 
       }
     });
   });
+}
+
+int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, int64_t* count) {
+  return ref_nodes(tree, -1, out, capacity, count);
 }
 
 int pptkg_tree_set_bucket(pptkg_tree* tree, int bucket, void* stream) {

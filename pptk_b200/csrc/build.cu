@@ -29,9 +29,10 @@ constexpr int TITEMS = TILE / BT;
 template <typename T, int D>
 struct Seg {
   int b, e;
-  int parent, side;
+  int parent, side;  // parent record and side; a cloud's root has parent = -1 - cloud
   int lvl;
   int rec;
+  long long n_orig;  // input rows of the segment's cloud (the reference's num_points)
   T lo[D], hi[D];  // loose extent (the reference's node_box), trimmed in place
   typename OrdOf<T>::type tlo[D], thi[D];
   int act;
@@ -42,13 +43,17 @@ struct Seg {
   int tile0, ntiles;
 };
 
+constexpr int MAX_LEVELS = 4096;  // grid-wide levels (segments above small_cap points)
+
 struct BuildCtl {
+  int status;
   int n_tiles;
-  int nB;
-  int nSmall;
+  int nsmall;
+  int small_next;
   int rec_count;
   int depth;
-  int status;
+  int level_cnt[MAX_LEVELS + 1];  // large segments per level
+  int rec_base[MAX_LEVELS + 1];
 };
 
 // ----------------------------------------------------------------- helpers
@@ -160,10 +165,51 @@ __global__ void k_compact(const T* __restrict__ in, int64_t n, const int* __rest
   soa.id[j] = (int)i;
 }
 
+// valid_off[c] = number of valid rows before cloud c (the stable compaction
+// keeps every cloud's valid rows together, in order).
+__global__ void k_cloud_off(const int* off, const int64_t* orig_off, int ncloud, int64_t* valid_off) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= ncloud) valid_off[c] = off[orig_off[c]];
+}
+
 // ------------------------------------------------------ grid-wide levels --
+// Level `lvl` works on list segs (ctl->level_cnt[lvl] entries).  Kernels are
+// launched with upper-bound grids and read the live counts from the device,
+// so the host never waits between levels.
 template <typename T, int D>
-__global__ void k_tiles(Seg<T, D>* segs, int nseg, int* tile_seg, BuildCtl* ctl) {
+__global__ void k_roots(const int64_t* valid_off, const int64_t* orig_off, int ncloud, int small_cap, Seg<T, D>* lvl0,
+                        Seg<T, D>* small, int small_capn, BuildCtl* ctl) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncloud) return;
+  const int b = (int)valid_off[c], e = (int)valid_off[c + 1];
+  if (e <= b) return;
+  Seg<T, D> g;
+  g.b = b;
+  g.e = e;
+  g.parent = -1 - c;
+  g.side = 0;
+  g.lvl = 0;
+  g.rec = -1;
+  g.n_orig = orig_off[c + 1] - orig_off[c];
+  for (int d = 0; d < D; d++) {
+    g.lo[d] = Limits<T>::max();  // replaced by the tight box at a root
+    g.hi[d] = Limits<T>::lowest();
+  }
+  if (e - b > small_cap) {
+    lvl0[atomicAdd(&ctl->level_cnt[0], 1)] = g;
+  } else {
+    const int slot = atomicAdd(&ctl->nsmall, 1);
+    if (slot < small_capn)
+      small[slot] = g;
+    else
+      atomicExch(&ctl->status, 7);
+  }
+}
+
+template <typename T, int D>
+__global__ void k_tiles(Seg<T, D>* segs, int lvl, int* tile_seg, BuildCtl* ctl) {
   __shared__ int sh[33];
+  const int nseg = ctl->level_cnt[lvl];
   int carry = 0;
   for (int c0 = 0; c0 < nseg; c0 += blockDim.x) {
     int i = c0 + threadIdx.x;
@@ -177,7 +223,11 @@ __global__ void k_tiles(Seg<T, D>* segs, int nseg, int* tile_seg, BuildCtl* ctl)
     }
     carry += tot;
   }
-  if (threadIdx.x == 0) ctl->n_tiles = carry;
+  if (threadIdx.x == 0) {
+    ctl->n_tiles = carry;
+    ctl->rec_base[lvl] = ctl->rec_count;
+    ctl->rec_count += nseg;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int i = wid; i < nseg; i += nw) {
@@ -198,9 +248,9 @@ __device__ __forceinline__ bool tile_range(const Seg<T, D>* segs, const int* til
 }
 
 template <typename T, int D>
-__global__ void k_seg_init(Seg<T, D>* segs, int nseg) {
+__global__ void k_seg_init(Seg<T, D>* segs, int lvl, const BuildCtl* ctl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nseg) return;
+  if (i >= ctl->level_cnt[lvl]) return;
   for (int d = 0; d < D; d++) {
     segs[i].tlo[d] = ord_of(Limits<T>::max());
     segs[i].thi[d] = ord_of(Limits<T>::lowest());
@@ -266,10 +316,10 @@ __global__ void __launch_bounds__(BT) k_bbox(Seg<T, D>* segs, const int* tile_se
 }
 
 template <typename T, int D>
-__global__ void k_node(Seg<T, D>* segs, int nseg, int rec_base, Rec<T, D>* recs, long long n_orig, int max_leaf,
-                       double thr) {
+__global__ void k_node(Seg<T, D>* segs, int lvl, BuildCtl* ctl, Rec<T, D>* recs, int rec_cap, int* root_rec,
+                       int max_leaf, double thr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nseg) return;
+  if (i >= ctl->level_cnt[lvl]) return;
   Seg<T, D>& g = segs[i];
   T tlo[D], thi[D], lo[D], hi[D];
   for (int d = 0; d < D; d++) {
@@ -281,16 +331,23 @@ __global__ void k_node(Seg<T, D>* segs, int nseg, int rec_base, Rec<T, D>* recs,
   Rec<T, D> rec;
   int act, sd = 0;
   T sv = (T)0;
-  node_logic<T, D>(g.e - g.b, n_orig, g.parent < 0, lo, hi, tlo, thi, max_leaf, thr, rec, act, sd, sv);
+  node_logic<T, D>(g.e - g.b, g.n_orig, g.parent < 0, lo, hi, tlo, thi, max_leaf, thr, rec, act, sd, sv);
   rec.begin = g.b;
   rec.end = g.e;
-  const int id = rec_base + i;
+  const int id = ctl->rec_base[lvl] + i;
+  if (id >= rec_cap) {
+    atomicExch(&ctl->status, 6);
+    g.act = 0;
+    return;
+  }
   recs[id] = rec;
   if (g.parent >= 0) {
     if (g.side == 0)
       recs[g.parent].left = id;
     else
       recs[g.parent].right = id;
+  } else {
+    root_rec[-g.parent - 1] = id;
   }
   g.rec = id;
   g.act = act;
@@ -360,8 +417,9 @@ __global__ void __launch_bounds__(BT) k_flags(int pass, Seg<T, D>* segs, const i
 }
 
 template <typename T, int D>
-__global__ void k_tscan(Seg<T, D>* segs, const long long* tile_cnt, long long* tile_off, BuildCtl* ctl) {
+__global__ void k_tscan(Seg<T, D>* segs, int lvl, const long long* tile_cnt, long long* tile_off, BuildCtl* ctl) {
   __shared__ long long sh[33];
+  if ((int)blockIdx.x >= ctl->level_cnt[lvl]) return;
   Seg<T, D>& g = segs[blockIdx.x];
   if (!g.act) return;
   long long carry = 0;
@@ -449,10 +507,10 @@ __global__ void __launch_bounds__(BT) k_swap(Seg<T, D>* segs, const int* tile_se
 }
 
 template <typename T, int D>
-__global__ void k_children(Seg<T, D>* segs, int nseg, Rec<T, D>* recs, Seg<T, D>* next, Seg<T, D>* small,
-                           int small_cap_pts, BuildCtl* ctl) {
+__global__ void k_children(Seg<T, D>* segs, int lvl, Rec<T, D>* recs, Seg<T, D>* next, Seg<T, D>* small,
+                           int small_capn, int small_cap_pts, BuildCtl* ctl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nseg) return;
+  if (i >= ctl->level_cnt[lvl]) return;
   const Seg<T, D>& g = segs[i];
   if (!g.act) return;
   const int count = g.e - g.b;
@@ -467,6 +525,8 @@ __global__ void k_children(Seg<T, D>* segs, int nseg, Rec<T, D>* recs, Seg<T, D>
     c.parent = g.rec;
     c.side = side;
     c.lvl = g.lvl + 1;
+    c.rec = -1;
+    c.n_orig = g.n_orig;
     for (int d = 0; d < D; d++) {
       c.lo[d] = g.lo[d];
       c.hi[d] = g.hi[d];
@@ -475,10 +535,15 @@ __global__ void k_children(Seg<T, D>* segs, int nseg, Rec<T, D>* recs, Seg<T, D>
       c.hi[g.sd] = g.sv;
     else
       c.lo[g.sd] = g.sv;
-    if (ce - cb > small_cap_pts)
-      next[atomicAdd(&ctl->nB, 1)] = c;
-    else
-      small[atomicAdd(&ctl->nSmall, 1)] = c;
+    if (ce - cb > small_cap_pts) {
+      next[atomicAdd(&ctl->level_cnt[lvl + 1], 1)] = c;
+    } else {
+      const int slot = atomicAdd(&ctl->nsmall, 1);
+      if (slot < small_capn)
+        small[slot] = c;
+      else
+        atomicExch(&ctl->status, 7);
+    }
   }
 }
 
@@ -491,15 +556,14 @@ struct Entry {
 
 constexpr int SUB_THREADS = 256;
 
-// Finishes one small segment's whole subtree in shared memory, one warp per
-// node, level by level.
+// Finishes small segments' whole subtrees in shared memory, one warp per
+// node, level by level.  Persistent: each CTA takes segments from the small
+// list until it is exhausted.
 template <typename T, int D>
 __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small, SoA<T, D> soa, Rec<T, D>* recs,
-                                                         int cap_pts, int cap_list, long long n_orig, int max_leaf,
+                                                         int* root_rec, int cap_pts, int cap_list, int max_leaf,
                                                          double thr, int rec_cap, BuildCtl* ctl) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const Seg<T, D> seg = small[blockIdx.x];
-  const int n = seg.e - seg.b;
   T* X[D];
   unsigned char* p = smem;
   for (int d = 0; d < D; d++) {
@@ -511,188 +575,206 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
   int* S = (int*)p;
   p += sizeof(int) * cap_pts;
   p = (unsigned char*)(((uintptr_t)p + 15) & ~(uintptr_t)15);
-  Entry<T, D>* LA = (Entry<T, D>*)p;
-  Entry<T, D>* LB = LA + cap_list;
-  int* cnt = (int*)(LB + cap_list);  // [0] nA, [1] nB, [2] base, [3] overflow
-
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    for (int d = 0; d < D; d++) X[d][i] = soa.x[d][seg.b + i];
-    ID[i] = soa.id[seg.b + i];
-  }
-  if (threadIdx.x == 0) {
-    Entry<T, D> r;
-    r.b = 0;
-    r.e = n;
-    r.parent = seg.parent;
-    r.side = seg.side;
-    for (int d = 0; d < D; d++) {
-      r.lo[d] = seg.lo[d];
-      r.hi[d] = seg.hi[d];
-    }
-    LA[0] = r;
-    cnt[0] = 1;
-    cnt[3] = 0;
-  }
-  __syncthreads();
+  Entry<T, D>* LA0 = (Entry<T, D>*)p;
+  Entry<T, D>* LB0 = LA0 + cap_list;
+  int* cnt = (int*)(LB0 + cap_list);  // [0] nA, [1] nB, [2] base, [3] overflow, [4] item
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  int levels = 0;
+  const int nsmall = min(ctl->nsmall, INT_MAX);
+
   while (true) {
-    const int nA = cnt[0];
-    if (nA == 0) break;
-    if (levels > n + 1) {  // every level splits ranges into strictly smaller ones
-      if (threadIdx.x == 0) atomicExch(&ctl->status, 5);
-      break;
+    if (threadIdx.x == 0) cnt[4] = atomicAdd(&ctl->small_next, 1);
+    __syncthreads();
+    const int item = cnt[4];
+    __syncthreads();
+    if (item >= nsmall) break;
+    const Seg<T, D> seg = small[item];
+    const int n = seg.e - seg.b;
+    Entry<T, D>* LA = LA0;
+    Entry<T, D>* LB = LB0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int d = 0; d < D; d++) X[d][i] = soa.x[d][seg.b + i];
+      ID[i] = soa.id[seg.b + i];
     }
     if (threadIdx.x == 0) {
-      cnt[1] = 0;
-      cnt[2] = atomicAdd(&ctl->rec_count, nA);
+      Entry<T, D> r;
+      r.b = 0;
+      r.e = n;
+      r.parent = seg.parent;
+      r.side = seg.side;
+      for (int d = 0; d < D; d++) {
+        r.lo[d] = seg.lo[d];
+        r.hi[d] = seg.hi[d];
+      }
+      LA[0] = r;
+      cnt[0] = 1;
+      cnt[3] = 0;
     }
     __syncthreads();
-    const int base = cnt[2];
-    levels++;
-    for (int ei = wid; ei < nA; ei += nw) {
-      Entry<T, D> en = LA[ei];
-      const int b = en.b, e = en.e, size = e - b;
-      T mn[D], mx[D];
-      for (int d = 0; d < D; d++) {
-        mn[d] = Limits<T>::max();
-        mx[d] = Limits<T>::lowest();
+    int levels = 0;
+    while (true) {
+      const int nA = cnt[0];
+      if (nA == 0) break;
+      if (levels > n + 1) {  // every level splits ranges into strictly smaller ones
+        if (threadIdx.x == 0) atomicExch(&ctl->status, 5);
+        break;
       }
-      for (int q = b + lane; q < e; q += 32)
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        cnt[1] = 0;
+        cnt[2] = atomicAdd(&ctl->rec_count, nA);
+      }
+      __syncthreads();
+      const int base = cnt[2];
+      levels++;
+      for (int ei = wid; ei < nA; ei += nw) {
+        Entry<T, D> en = LA[ei];
+        const int b = en.b, e = en.e, size = e - b;
+        T mn[D], mx[D];
         for (int d = 0; d < D; d++) {
-          T v = X[d][q];
-          mn[d] = min(mn[d], v);
-          mx[d] = max(mx[d], v);
+          mn[d] = Limits<T>::max();
+          mx[d] = Limits<T>::lowest();
         }
-      for (int d = 0; d < D; d++) {
-        mn[d] = warp_min(mn[d]);
-        mx[d] = warp_max(mx[d]);
-      }
-      int act = 0, sd = 0;
-      T sv = (T)0;
-      const int id = base + ei;
-      if (lane == 0) {
-        Rec<T, D> rec;
-        node_logic<T, D>(size, n_orig, en.parent < 0, en.lo, en.hi, mn, mx, max_leaf, thr, rec, act, sd, sv);
-        rec.begin = seg.b + b;
-        rec.end = seg.b + e;
-        if (id >= rec_cap) {
-          atomicExch(&ctl->status, 6);
-          act = 0;
-        } else {
-          recs[id] = rec;
-        }
-        if (en.parent >= 0 && id < rec_cap) {
-          if (en.side == 0)
-            recs[en.parent].left = id;
-          else
-            recs[en.parent].right = id;
-        }
-        LA[ei] = en;  // keep the trimmed extent for the children
-      }
-      act = __shfl_sync(0xffffffffu, act, 0);
-      if (!act) continue;
-      sd = __shfl_sync(0xffffffffu, sd, 0);
-      sv = __shfl_sync(0xffffffffu, sv, 0);
-      T* v = X[sd];
-      int L1 = 0, L2 = 0;
-      for (int q0 = b; q0 < e; q0 += 32) {
-        int q = q0 + lane;
-        T x = q < e ? v[q] : sv;
-        bool in = q < e;
-        L1 += __popc(__ballot_sync(0xffffffffu, in && x < sv));
-        L2 += __popc(__ballot_sync(0xffffffffu, in && x <= sv));
-      }
-      const int half = size / 2;
-      for (int pass = 1; pass <= 2; pass++) {
-        const int zlo = pass == 1 ? b : b + L1;
-        const int Z = pass == 1 ? b + L1 : b + L2;
-        int G = 0;
-        for (int q0 = zlo; q0 < Z; q0 += 32) {
-          int q = q0 + lane;
-          bool f = false;
-          if (q < Z) {
-            T x = v[q];
-            f = pass == 1 ? !(x < sv) : (x > sv);
-          }
-          unsigned bal = __ballot_sync(0xffffffffu, f);
-          if (f) S[b + G + __popc(bal & lt)] = q;
-          G += __popc(bal);
-        }
-        int a = 0;
-        for (int q0 = Z; q0 < e; q0 += 32) {
-          int q = q0 + lane;
-          bool f = false;
-          if (q < e) {
-            T x = v[q];
-            f = pass == 1 ? (x < sv) : (x <= sv);
-          }
-          unsigned bal = __ballot_sync(0xffffffffu, f);
-          if (f) {
-            int r = a + __popc(bal & lt);
-            if (r < G) S[b + half + (G - 1 - r)] = q;
-          }
-          a += __popc(bal);
-        }
-        if (a != G && lane == 0) atomicExch(&ctl->status, 2);
-        __syncwarp();
-        for (int j = lane; j < G; j += 32) {
-          int x = S[b + j], y = S[b + half + j];
+        for (int q = b + lane; q < e; q += 32)
           for (int d = 0; d < D; d++) {
-            T t = X[d][x];
-            X[d][x] = X[d][y];
-            X[d][y] = t;
+            T v = X[d][q];
+            mn[d] = min(mn[d], v);
+            mx[d] = max(mx[d], v);
           }
-          int t = ID[x];
-          ID[x] = ID[y];
-          ID[y] = t;
+        for (int d = 0; d < D; d++) {
+          mn[d] = warp_min(mn[d]);
+          mx[d] = warp_max(mx[d]);
         }
-        __syncwarp();
-      }
-      if (lane == 0) {
-        const int si = b + num_left_rule(L1, L2, size);
-        if (id < rec_cap) recs[id].split_index = seg.b + si;
-        const Entry<T, D> par = LA[ei];
-        for (int side = 0; side < 2; side++) {
-          int cb = side ? si : b, ce = side ? e : si;
-          if (cb >= ce) continue;
-          Entry<T, D> c;
-          c.b = cb;
-          c.e = ce;
-          c.parent = id;
-          c.side = side;
-          for (int d = 0; d < D; d++) {
-            c.lo[d] = par.lo[d];
-            c.hi[d] = par.hi[d];
+        int act = 0, sd = 0;
+        T sv = (T)0;
+        const int id = base + ei;
+        if (lane == 0) {
+          Rec<T, D> rec;
+          node_logic<T, D>(size, seg.n_orig, en.parent < 0, en.lo, en.hi, mn, mx, max_leaf, thr, rec, act, sd, sv);
+          rec.begin = seg.b + b;
+          rec.end = seg.b + e;
+          if (id >= rec_cap) {
+            atomicExch(&ctl->status, 6);
+            act = 0;
+          } else {
+            recs[id] = rec;
+            if (en.parent >= 0) {
+              if (en.side == 0)
+                recs[en.parent].left = id;
+              else
+                recs[en.parent].right = id;
+            } else {
+              root_rec[-en.parent - 1] = id;
+            }
           }
-          if (side == 0)
-            c.hi[sd] = sv;
-          else
-            c.lo[sd] = sv;
-          int slot = atomicAdd(&cnt[1], 1);
-          if (slot < cap_list)
-            LB[slot] = c;
-          else
-            atomicExch(&cnt[3], 1);
+          LA[ei] = en;  // keep the trimmed extent for the children
+        }
+        act = __shfl_sync(0xffffffffu, act, 0);
+        if (!act) continue;
+        sd = __shfl_sync(0xffffffffu, sd, 0);
+        sv = __shfl_sync(0xffffffffu, sv, 0);
+        T* v = X[sd];
+        int L1 = 0, L2 = 0;
+        for (int q0 = b; q0 < e; q0 += 32) {
+          int q = q0 + lane;
+          T x = q < e ? v[q] : sv;
+          bool in = q < e;
+          L1 += __popc(__ballot_sync(0xffffffffu, in && x < sv));
+          L2 += __popc(__ballot_sync(0xffffffffu, in && x <= sv));
+        }
+        const int half = size / 2;
+        for (int pass = 1; pass <= 2; pass++) {
+          const int zlo = pass == 1 ? b : b + L1;
+          const int Z = pass == 1 ? b + L1 : b + L2;
+          int G = 0;
+          for (int q0 = zlo; q0 < Z; q0 += 32) {
+            int q = q0 + lane;
+            bool f = false;
+            if (q < Z) {
+              T x = v[q];
+              f = pass == 1 ? !(x < sv) : (x > sv);
+            }
+            unsigned bal = __ballot_sync(0xffffffffu, f);
+            if (f && G + __popc(bal & lt) < half) S[b + G + __popc(bal & lt)] = q;
+            G += __popc(bal);
+          }
+          int a = 0;
+          for (int q0 = Z; q0 < e; q0 += 32) {
+            int q = q0 + lane;
+            bool f = false;
+            if (q < e) {
+              T x = v[q];
+              f = pass == 1 ? (x < sv) : (x <= sv);
+            }
+            unsigned bal = __ballot_sync(0xffffffffu, f);
+            if (f) {
+              int r = a + __popc(bal & lt);
+              if (r < G && G <= half) S[b + half + (G - 1 - r)] = q;
+            }
+            a += __popc(bal);
+          }
+          if ((a != G || G > half) && lane == 0) atomicExch(&ctl->status, 2);
+          __syncwarp();
+          if (a == G && G <= half)
+            for (int j = lane; j < G; j += 32) {
+              int x = S[b + j], y = S[b + half + j];
+              for (int d = 0; d < D; d++) {
+                T t = X[d][x];
+                X[d][x] = X[d][y];
+                X[d][y] = t;
+              }
+              int t = ID[x];
+              ID[x] = ID[y];
+              ID[y] = t;
+            }
+          __syncwarp();
+        }
+        if (lane == 0) {
+          const int si = b + num_left_rule(L1, L2, size);
+          if (id < rec_cap) recs[id].split_index = seg.b + si;
+          const Entry<T, D> par = LA[ei];
+          for (int side = 0; side < 2; side++) {
+            int cb = side ? si : b, ce = side ? e : si;
+            if (cb >= ce) continue;
+            Entry<T, D> c;
+            c.b = cb;
+            c.e = ce;
+            c.parent = id;
+            c.side = side;
+            for (int d = 0; d < D; d++) {
+              c.lo[d] = par.lo[d];
+              c.hi[d] = par.hi[d];
+            }
+            if (side == 0)
+              c.hi[sd] = sv;
+            else
+              c.lo[sd] = sv;
+            int slot = atomicAdd(&cnt[1], 1);
+            if (slot < cap_list)
+              LB[slot] = c;
+            else
+              atomicExch(&cnt[3], 1);
+          }
         }
       }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        cnt[0] = min(cnt[1], cap_list);
+        if (cnt[3]) atomicExch(&ctl->status, 3);
+      }
+      __syncthreads();
+      Entry<T, D>* tmp = LA;
+      LA = LB;
+      LB = tmp;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      cnt[0] = min(cnt[1], cap_list);
-      if (cnt[3]) atomicExch(&ctl->status, 3);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int d = 0; d < D; d++) soa.x[d][seg.b + i] = X[d][i];
+      soa.id[seg.b + i] = ID[i];
     }
+    if (threadIdx.x == 0) atomicMax(&ctl->depth, seg.lvl + levels);
     __syncthreads();
-    Entry<T, D>* tmp = LA;
-    LA = LB;
-    LB = tmp;
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    for (int d = 0; d < D; d++) soa.x[d][seg.b + i] = X[d][i];
-    soa.id[seg.b + i] = ID[i];
-  }
-  if (threadIdx.x == 0) atomicMax(&ctl->depth, seg.lvl + levels);
 }
 
 // ------------------------------------------------------- finishing ----
@@ -735,39 +817,48 @@ __global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, cons
   nodes[tid[i]] = t;
 }
 
-// Root-is-a-bucket tree (or empty tree): a single node whose first child is
-// the whole point range.
+// Per-cloud traversal roots: the root record's node when it is an inner
+// node, otherwise a dedicated node (index nt + c) whose first child is the
+// whole cloud as one bucket (or nothing, for a cloud without valid points).
 template <typename T, int D>
-__global__ void k_tsingle(const Rec<T, D>* recs, int n_recs, int nv, TNode<T, D>* nodes) {
-  TNode<T, D> t;
-  for (int c = 0; c < 2; c++)
-    for (int d = 0; d < D; d++) {
-      t.lo[c][d] = Limits<T>::max();
-      t.hi[c][d] = Limits<T>::lowest();
-    }
-  t.ref[0] = -1;
-  t.ref[1] = -1;
-  t.cnt[0] = 0;
-  t.cnt[1] = 0;
-  if (n_recs > 0 && nv > 0) {
-    for (int d = 0; d < D; d++) {
-      t.lo[0][d] = recs[0].lo[d];
-      t.hi[0][d] = recs[0].hi[d];
-    }
-    t.cnt[0] = nv;
+__global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64_t* valid_off, int ncloud,
+                         const int* flag, const int* tid, int nt, TNode<T, D>* nodes, int* root_tnode) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncloud) return;
+  const int r = root_rec[c];
+  if (r >= 0 && flag[r]) {
+    root_tnode[c] = tid[r];
+    return;
   }
-  nodes[0] = t;
+  TNode<T, D> t;
+  for (int k = 0; k < 2; k++)
+    for (int d = 0; d < D; d++) {
+      t.lo[k][d] = Limits<T>::max();
+      t.hi[k][d] = Limits<T>::lowest();
+    }
+  t.ref[0] = t.ref[1] = -1;
+  t.cnt[0] = t.cnt[1] = 0;
+  if (r >= 0) {
+    for (int d = 0; d < D; d++) {
+      t.lo[0][d] = recs[r].lo[d];
+      t.hi[0][d] = recs[r].hi[d];
+    }
+    t.ref[0] = -(int)valid_off[c] - 1;
+    t.cnt[0] = (int)(valid_off[c + 1] - valid_off[c]);
+  }
+  nodes[nt + c] = t;
+  root_tnode[c] = nt + c;
 }
 
 // ------------------------------------------------------------ host side ----
 template <typename T, int D>
 int small_capacity(int max_leaf, int& cap_list, size_t& smem) {
-  const size_t budget = 160 * 1024;
-  int cap = sizeof(T) == 4 ? 4096 : 2048;
+  const size_t budget = 72 * 1024;
+  int cap = sizeof(T) == 4 ? 2048 : 1024;
   while (true) {
     cap_list = 2 * (cap / (max_leaf + 1)) + 2;
     smem = (sizeof(T) * D + 2 * sizeof(int)) * (size_t)cap + 16 + 2 * sizeof(Entry<T, D>) * (size_t)cap_list +
-           4 * sizeof(int);
+           8 * sizeof(int);
     if (smem <= budget || cap <= 64) break;
     cap /= 2;
   }
@@ -775,8 +866,10 @@ int small_capacity(int max_leaf, int& cap_list, size_t& smem) {
 }
 
 template <typename T, int D>
-TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int bucket, cudaStream_t st) {
-  if (n > (int64_t)INT32_MAX - 1) throw Error(E_INVALID, "k-d tree supports at most 2^31-2 points");
+TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int ncloud, int max_leaf, double thr,
+                       int bucket, cudaStream_t st) {
+  if (n > (int64_t)INT32_MAX / 2 - 64) throw Error(E_INVALID, "k-d tree supports at most 2^30 points");
+  if (ncloud < 1) throw Error(E_INVALID, "at least one cloud");
   if (max_leaf < 1) max_leaf = 1;
   Stage stage("build", st);
   keep_pool_cached(st);
@@ -788,19 +881,35 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
   tree->max_leaf = max_leaf;
   tree->empty_split = thr;
   tree->bucket = bucket;
+  tree->ncloud = ncloud;
   PPTKG_CUDA(cudaGetDevice(&tree->device));
+  tree->orig_off_h.assign(orig_off_h, orig_off_h + ncloud + 1);
+  if (tree->orig_off_h[0] != 0 || tree->orig_off_h[ncloud] != n)
+    throw Error(E_INVALID, "cloud offsets must start at 0 and end at n");
+  for (int c = 0; c < ncloud; c++)
+    if (tree->orig_off_h[c + 1] < tree->orig_off_h[c]) throw Error(E_INVALID, "cloud offsets must not decrease");
+  PPTKG_CUDA(cudaMallocAsync((void**)&tree->orig_off, sizeof(int64_t) * (ncloud + 1), st));
+  PPTKG_CUDA(cudaMallocAsync((void**)&tree->valid_off, sizeof(int64_t) * (ncloud + 1), st));
+  PPTKG_CUDA(cudaMallocAsync((void**)&tree->root_rec, sizeof(int) * ncloud, st));
+  PPTKG_CUDA(cudaMallocAsync((void**)&tree->root_tnode, sizeof(int) * ncloud, st));
+  PPTKG_CUDA(cudaMemcpyAsync(tree->orig_off, orig_off_h, sizeof(int64_t) * (ncloud + 1), cudaMemcpyHostToDevice, st));
+  PPTKG_CUDA(cudaMemsetAsync(tree->root_rec, 0xff, sizeof(int) * ncloud, st));
 
-  // valid-point compaction (ValidPointIndices, kdtree-impl.h:53-75)
+  // valid-point compaction (ValidPointIndices, kdtree-impl.h:53-75), per cloud
+  std::unique_ptr<Stage> st_prep(new Stage("build.prep", st));
   DevBuf<int> flag(n + 1, st), off(n + 1, st);
-  int* d_nv_ptr = off.get() + n;
   if (n > 0) {
     k_valid<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get());
     PPTKG_CHECK_LAUNCH();
   }
-  exclusive_scan<int, int>(flag.get(), off.get(), n, d_nv_ptr, st);
-  int nv = 0;
-  PPTKG_CUDA(cudaMemcpyAsync(&nv, d_nv_ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  exclusive_scan<int, int>(flag.get(), off.get(), n, off.get() + n, st);
+  k_cloud_off<<<div_up(ncloud + 1, 256), 256, 0, st>>>(off.get(), tree->orig_off, ncloud, tree->valid_off);
+  PPTKG_CHECK_LAUNCH();
+  tree->valid_off_h.resize(ncloud + 1);
+  PPTKG_CUDA(cudaMemcpyAsync(tree->valid_off_h.data(), tree->valid_off, sizeof(int64_t) * (ncloud + 1),
+                             cudaMemcpyDeviceToHost, st));
   PPTKG_CUDA(cudaStreamSynchronize(st));
+  const int nv = (int)tree->valid_off_h[ncloud];
   tree->nv = nv;
 
   DevBuf<T> xs((size_t)D * nv + 1, st);
@@ -814,135 +923,117 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
   }
   flag.release();
   off.release();
+  st_prep.reset();
 
   int cap_list;
   size_t smem;
   const int small_cap = small_capacity<T, D>(max_leaf, cap_list, smem);
-
-  // records: every node is a disjoint range at its level; nodes with children
-  // have > max_leaf points, so the count is below 2 * nv / (max_leaf + 1) + depth.
-  // every record is a non-empty range and every split has two children, so a
-  // binary tree over nv points has at most 2 * nv - 1 records
+  // a binary tree over nv points has at most 2 nv - 1 records
   const size_t rec_cap = 2 * (size_t)nv + 64;
   DevBuf<Rec<T, D>> recbuf(rec_cap, st);
   Rec<T, D>* recs = recbuf.get();
 
-  DevBuf<BuildCtl> ctl(1, st);
-  PPTKG_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(BuildCtl), st));
-  BuildCtl hctl;
-
-  Seg<T, D> root;
-  memset(&root, 0, sizeof(root));
-  root.b = 0;
-  root.e = nv;
-  root.parent = -1;
-  root.side = 0;
-  root.lvl = 0;
-  for (int d = 0; d < D; d++) {
-    root.lo[d] = Limits<T>::max();  // replaced by the tight box at the root
-    root.hi[d] = Limits<T>::lowest();
-  }
-
-  size_t small_cap_n = 1024;
-  DevBuf<Seg<T, D>> smallL(small_cap_n, st);
-  int nSmall = 0;
+  // large segments per level are disjoint and above small_cap points
+  const int seg_cap = nv / (small_cap + 1) + 2;
+  const int max_tiles = nv / TILE + seg_cap + 2;
+  int small_capn = ncloud + 2 * 64 * (seg_cap + 1);
   int depth = 0;
-  if (nv > 0) {
-    if (nv > small_cap) {
-      Stage st_levels("build.levels", st);
-      DevBuf<Seg<T, D>> segA(1, st), segB;
-      PPTKG_CUDA(cudaMemcpyAsync(segA.get(), &root, sizeof(root), cudaMemcpyHostToDevice, st));
-      int nA = 1;
-      int rec_base = 0;
-      DevBuf<int> blpos(nv, st), grpos(nv, st);
-      size_t tile_cap = 0;
-      DevBuf<int> tile_seg;
-      DevBuf<long long> tile_cnt, tile_off;
-      int lvl = 0;
-      while (nA > 0) {
-        const size_t max_tiles = (size_t)nv / TILE + (size_t)nA + 1;
-        if (max_tiles > tile_cap) {
-          tile_cap = max_tiles * 2;
-          tile_seg.alloc(tile_cap, st);
-          tile_cnt.alloc(tile_cap, st);
-          tile_off.alloc(tile_cap, st);
-        }
-        if ((size_t)nSmall + 2 * (size_t)nA > small_cap_n) {
-          size_t nc = std::max(small_cap_n * 2, (size_t)nSmall + 2 * (size_t)nA);
-          DevBuf<Seg<T, D>> bigger(nc, st);
-          if (nSmall)
-            PPTKG_CUDA(cudaMemcpyAsync(bigger.get(), smallL.get(), nSmall * sizeof(Seg<T, D>),
-                                       cudaMemcpyDeviceToDevice, st));
-          std::swap(bigger.p, smallL.p);
-          std::swap(bigger.n, smallL.n);
-          small_cap_n = nc;
-        }
-        segB.alloc(2 * (size_t)nA, st);
-        const unsigned gt = (unsigned)max_tiles;
-        k_tiles<T, D><<<1, 1024, 0, st>>>(segA.get(), nA, tile_seg.get(), ctl.get());
-        PPTKG_CHECK_LAUNCH();
-        k_seg_init<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA);
-        PPTKG_CHECK_LAUNCH();
-        k_bbox<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa);
-        PPTKG_CHECK_LAUNCH();
-        k_node<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA, rec_base, recs, (long long)n, max_leaf, thr);
-        PPTKG_CHECK_LAUNCH();
-        k_count<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa);
-        PPTKG_CHECK_LAUNCH();
-        for (int pass = 1; pass <= 2; pass++) {
-          k_flags<T, D><<<gt, BT, 0, st>>>(pass, segA.get(), tile_seg.get(), ctl.get(), soa, tile_cnt.get());
-          PPTKG_CHECK_LAUNCH();
-          k_tscan<T, D><<<nA, 256, 0, st>>>(segA.get(), tile_cnt.get(), tile_off.get(), ctl.get());
-          PPTKG_CHECK_LAUNCH();
-          k_scatter<T, D><<<gt, BT, 0, st>>>(pass, segA.get(), tile_seg.get(), ctl.get(), soa, tile_off.get(),
-                                            blpos.get(), grpos.get());
-          PPTKG_CHECK_LAUNCH();
-          k_swap<T, D><<<gt, BT, 0, st>>>(segA.get(), tile_seg.get(), ctl.get(), soa, blpos.get(), grpos.get());
-          PPTKG_CHECK_LAUNCH();
-        }
-        PPTKG_CUDA(cudaMemsetAsync(&ctl.get()->nB, 0, sizeof(int), st));
-        k_children<T, D><<<div_up(nA, 128), 128, 0, st>>>(segA.get(), nA, recs, segB.get(), smallL.get(), small_cap,
-                                                          ctl.get());
-        PPTKG_CHECK_LAUNCH();
-        PPTKG_CUDA(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(BuildCtl), cudaMemcpyDeviceToHost, st));
-        PPTKG_CUDA(cudaStreamSynchronize(st));
-        if (hctl.status) throw Error(E_DEVICE, "device build: partition check failed");
-        rec_base += nA;
-        nSmall = hctl.nSmall;
-        nA = hctl.nB;
-        if (lvl > nv) throw Error(E_DEVICE, "device build: level count exceeds the point count");
-        std::swap(segA.p, segB.p);
-        std::swap(segA.n, segB.n);
-        lvl++;
-      }
-      depth = lvl;
-      PPTKG_CUDA(cudaMemcpyAsync(&ctl.get()->rec_count, &rec_base, sizeof(int), cudaMemcpyHostToDevice, st));
-    } else {
-      PPTKG_CUDA(cudaMemcpyAsync(smallL.get(), &root, sizeof(root), cudaMemcpyHostToDevice, st));
-      nSmall = 1;
-    }
-    if (nSmall > 0) {
-      Stage st_sub("build.subtree", st);
-      PPTKG_CUDA(cudaFuncSetAttribute(k_subtree<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_subtree<T, D><<<nSmall, SUB_THREADS, smem, st>>>(smallL.get(), soa, recs, small_cap, cap_list, (long long)n,
-                                                         max_leaf, thr, (int)rec_cap, ctl.get());
+  for (int attempt = 0; attempt < 4; attempt++, small_capn *= 4) {
+    Stage st_att("build.attempt", st);
+    DevBuf<BuildCtl> ctl(1, st);
+    PPTKG_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(BuildCtl), st));
+    DevBuf<Seg<T, D>> segL[2] = {DevBuf<Seg<T, D>>(seg_cap, st), DevBuf<Seg<T, D>>(seg_cap, st)};
+    DevBuf<Seg<T, D>> smallL(small_capn, st);
+    if (nv > 0) {
+      k_roots<T, D><<<div_up(ncloud, 128), 128, 0, st>>>(tree->valid_off, tree->orig_off, ncloud, small_cap,
+                                                          segL[0].get(), smallL.get(), small_capn, ctl.get());
       PPTKG_CHECK_LAUNCH();
     }
+    int levels = 0;
+    {
+      Stage st_levels("build.levels", st);
+      DevBuf<int> blpos(nv + 1, st), grpos(nv + 1, st);
+      DevBuf<int> tile_seg(max_tiles, st);
+      DevBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
+      const unsigned gt = (unsigned)max_tiles;
+      const unsigned gs = (unsigned)div_up(seg_cap, 128);
+      int h0 = 0;
+      if (nv > 0) {
+        PPTKG_CUDA(cudaMemcpyAsync(&h0, &ctl.get()->level_cnt[0], sizeof(int), cudaMemcpyDeviceToHost, st));
+        PPTKG_CUDA(cudaStreamSynchronize(st));
+      }
+      for (int lvl = 0; h0 > 0 && lvl < MAX_LEVELS; lvl++) {
+        Seg<T, D>* A = segL[lvl & 1].get();
+        Seg<T, D>* B = segL[(lvl + 1) & 1].get();
+        k_tiles<T, D><<<1, 1024, 0, st>>>(A, lvl, tile_seg.get(), ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        k_seg_init<T, D><<<gs, 128, 0, st>>>(A, lvl, ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        k_bbox<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa);
+        PPTKG_CHECK_LAUNCH();
+        k_node<T, D><<<gs, 128, 0, st>>>(A, lvl, ctl.get(), recs, (int)rec_cap, tree->root_rec, max_leaf, thr);
+        PPTKG_CHECK_LAUNCH();
+        k_count<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa);
+        PPTKG_CHECK_LAUNCH();
+        for (int pass = 1; pass <= 2; pass++) {
+          k_flags<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_cnt.get());
+          PPTKG_CHECK_LAUNCH();
+          k_tscan<T, D><<<(unsigned)seg_cap, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
+          PPTKG_CHECK_LAUNCH();
+          k_scatter<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_off.get(), blpos.get(),
+                                            grpos.get());
+          PPTKG_CHECK_LAUNCH();
+          k_swap<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa, blpos.get(), grpos.get());
+          PPTKG_CHECK_LAUNCH();
+        }
+        k_children<T, D><<<gs, 128, 0, st>>>(A, lvl, recs, B, smallL.get(), small_capn, small_cap, ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        levels = lvl + 1;
+        // the host looks at the next level's size every fourth level only;
+        // kernels of a level without segments exit at once
+        if (levels % 4 == 0) {
+          int h = 0;
+          PPTKG_CUDA(cudaMemcpyAsync(&h, &ctl.get()->level_cnt[lvl + 1], sizeof(int), cudaMemcpyDeviceToHost, st));
+          PPTKG_CUDA(cudaStreamSynchronize(st));
+          if (h == 0) break;
+        }
+      }
+    }
+    BuildCtl hctl;
     PPTKG_CUDA(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(BuildCtl), cudaMemcpyDeviceToHost, st));
     PPTKG_CUDA(cudaStreamSynchronize(st));
-    if (hctl.status) throw Error(E_DEVICE, "device build: subtree check failed (code " + std::to_string(hctl.status) + ")");
-    if ((size_t)hctl.rec_count > rec_cap) throw Error(E_DEVICE, "device build: record capacity exceeded");
+    if (hctl.status == 7) continue;  // small list too short: retry with more room
+    if (hctl.status) throw Error(E_DEVICE, "device build: partition check failed (code " + std::to_string(hctl.status) + ")");
+    if (levels >= MAX_LEVELS) throw Error(E_DEVICE, "device build: more than 4096 levels of large nodes");
+    depth = levels;
+    if (hctl.nsmall > 0) {
+      Stage st_sub("build.subtree", st);
+      PPTKG_CUDA(cudaFuncSetAttribute(k_subtree<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int per_sm = 1, nsm = 1;
+      PPTKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subtree<T, D>, SUB_THREADS, smem));
+      PPTKG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, tree->device));
+      const int grid = std::max(1, std::min(hctl.nsmall, std::max(per_sm, 1) * nsm));
+      k_subtree<T, D><<<grid, SUB_THREADS, smem, st>>>(smallL.get(), soa, recs, tree->root_rec, small_cap, cap_list,
+                                                       max_leaf, thr, (int)rec_cap, ctl.get());
+      PPTKG_CHECK_LAUNCH();
+      PPTKG_CUDA(cudaMemcpyAsync(&hctl, ctl.get(), sizeof(BuildCtl), cudaMemcpyDeviceToHost, st));
+      PPTKG_CUDA(cudaStreamSynchronize(st));
+      if (hctl.status)
+        throw Error(E_DEVICE, "device build: subtree check failed (code " + std::to_string(hctl.status) + ")");
+    }
     tree->n_recs = hctl.rec_count;
     depth = std::max(depth, hctl.depth);
+    break;
   }
+  if ((size_t)tree->n_recs > rec_cap) throw Error(E_DEVICE, "device build: record capacity exceeded");
   tree->depth = depth;
   PPTKG_CUDA(cudaMallocAsync(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>), st));
   if (tree->n_recs)
     PPTKG_CUDA(cudaMemcpyAsync(tree->recs, recs, tree->n_recs * sizeof(Rec<T, D>), cudaMemcpyDeviceToDevice, st));
-  recs = (Rec<T, D>*)tree->recs;
   recbuf.release();
 
   // tree-ordered points and the forward map
+  std::unique_ptr<Stage> st_fin(new Stage("build.finish", st));
   PointRec<T, D>* pts = nullptr;
   PPTKG_CUDA(cudaMallocAsync((void**)&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>), st));
   tree->pts = pts;
@@ -953,21 +1044,32 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
     PPTKG_CHECK_LAUNCH();
   }
 
+  st_fin.reset();
   // traversal hierarchy cut at `bucket` points
-  make_tnodes<T, D>(tree.get(), bucket, st);
+  {
+    Stage st_tn("build.tnodes", st);
+    make_tnodes<T, D>(tree.get(), bucket, st);
+  }
 
-  if (nv > 0) {
-    Rec<T, D> r0;
-    PPTKG_CUDA(cudaMemcpyAsync(&r0, recs, sizeof(r0), cudaMemcpyDeviceToHost, st));
+  Rec<T, D> r0;
+  int root0 = -1;
+  PPTKG_CUDA(cudaMemcpyAsync(&root0, tree->root_rec, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (root0 >= 0) {
+    PPTKG_CUDA(cudaMemcpyAsync(&r0, (Rec<T, D>*)tree->recs + root0, sizeof(r0), cudaMemcpyDeviceToHost, st));
     PPTKG_CUDA(cudaStreamSynchronize(st));
     for (int d = 0; d < D; d++) {
       tree->root_lo[d] = (double)r0.lo[d];
       tree->root_hi[d] = (double)r0.hi[d];
     }
-  } else {
-    PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   return tree.release();
+}
+
+template <typename T, int D>
+TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int bucket, cudaStream_t st) {
+  const int64_t off[2] = {0, n};
+  return build_forest<T, D>(d_in, n, off, 1, max_leaf, thr, bucket, st);
 }
 
 template <typename T, int D>
@@ -990,15 +1092,20 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
     PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   TNode<T, D>* nodes = nullptr;
-  PPTKG_CUDA(cudaMallocAsync((void**)&nodes, std::max(nt, 1) * sizeof(TNode<T, D>), st));
+  PPTKG_CUDA(cudaMallocAsync((void**)&nodes, (size_t)(nt + tree->ncloud) * sizeof(TNode<T, D>), st));
   tree->tnodes = nodes;
-  tree->n_tnodes = std::max(nt, 1);
+  tree->n_tnodes = nt + tree->ncloud;
   if (nt > 0) {
     k_tfill<T, D><<<div_up(nr, 256), 256, 0, st>>>(recs, nr, flag.get(), tid.get(), nodes);
-  } else {
-    k_tsingle<T, D><<<1, 1, 0, st>>>(recs, nr, (int)tree->nv, nodes);
+    PPTKG_CHECK_LAUNCH();
   }
+  k_troots<T, D><<<div_up(tree->ncloud, 128), 128, 0, st>>>(recs, tree->root_rec, tree->valid_off, tree->ncloud,
+                                                            nr > 0 ? flag.get() : nullptr, tid.get(), nt, nodes,
+                                                            tree->root_tnode);
   PPTKG_CHECK_LAUNCH();
+  tree->root_tnode_h.resize(tree->ncloud);
+  PPTKG_CUDA(cudaMemcpyAsync(tree->root_tnode_h.data(), tree->root_tnode, sizeof(int) * tree->ncloud,
+                             cudaMemcpyDeviceToHost, st));
   tree->tdepth = tree->depth + 2;
   PPTKG_CUDA(cudaStreamSynchronize(st));
 }
@@ -1015,10 +1122,15 @@ TreeBase::~TreeBase() {
   if (recs) cudaFreeAsync(recs, stream);
   if (tnodes) cudaFreeAsync(tnodes, stream);
   if (fwd) cudaFreeAsync(fwd, stream);
+  if (root_rec) cudaFreeAsync(root_rec, stream);
+  if (root_tnode) cudaFreeAsync(root_tnode, stream);
+  if (valid_off) cudaFreeAsync(valid_off, stream);
+  if (orig_off) cudaFreeAsync(orig_off, stream);
 }
 
-#define PPTKG_INST_BUILD(T, D)                                                                         \
-  template TreeBase* build_tree<T, D>(const T*, int64_t, int, double, int, cudaStream_t);             \
+#define PPTKG_INST_BUILD(T, D)                                                                                  \
+  template TreeBase* build_tree<T, D>(const T*, int64_t, int, double, int, cudaStream_t);                      \
+  template TreeBase* build_forest<T, D>(const T*, int64_t, const int64_t*, int, int, double, int, cudaStream_t); \
   template void make_tnodes<T, D>(TreeBase*, int, cudaStream_t);
 
 PPTKG_INST_BUILD(float, 3)

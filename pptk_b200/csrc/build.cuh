@@ -19,6 +19,14 @@ struct SoA {
 template <typename T, int D>
 TreeBase* build_tree(const T* d_points, int64_t n, int max_leaf, double empty_split, int bucket, cudaStream_t st);
 
+// Builds one tree per cloud over the consecutive row ranges
+// [orig_off[c], orig_off[c+1]) of the same point array (host offsets,
+// ncloud + 1 entries), each exactly the tree the reference builds for that
+// cloud alone.
+template <typename T, int D>
+TreeBase* build_forest(const T* d_points, int64_t n, const int64_t* orig_off_h, int ncloud, int max_leaf,
+                       double empty_split, int bucket, cudaStream_t st);
+
 // (Re)derives the traversal hierarchy for a bucket size.
 template <typename T, int D>
 void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st);

@@ -244,7 +244,7 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
     }
     sp++;
   };
-  TNode<T, D> nd = load_node(tv.nodes, 0);
+  TNode<T, D> nd = load_node(tv.nodes, tv.root);
   while (true) {
     if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
       ok = false;
@@ -330,7 +330,7 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
   int sp = 0;
-  int cur = 0;
+  int cur = tv.root;
   bool ok = true;
   auto scan = [&](int begin, int cnt, bool mine) {
     for (int base = begin; base < begin + cnt; base += 32) {

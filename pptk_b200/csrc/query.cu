@@ -23,6 +23,7 @@ TreeView<T, D> view_of(const TreeBase* t) {
   v.nv = (int)t->nv;
   v.depth = t->tdepth;
   v.n_nodes = t->n_tnodes;
+  v.root = t->root_tnode_h.empty() ? 0 : t->root_tnode_h[0];
   return v;
 }
 
@@ -107,7 +108,7 @@ __global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
   DistT p[D];
 #pragma unroll
   for (int d = 0; d < D; d++) p[d] = (DistT)q[(int64_t)i * D + d];
-  int cur = 0, k = 0;
+  int cur = tv.root, k = 0;
   for (int step = 0; step <= tv.depth + 1; step++) {
     const TNode<T, D>& nd = tv.nodes[cur];
     int c;

@@ -20,6 +20,8 @@
 // tighter boxes change the amount of work, never an answer.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace pptkg {
@@ -58,9 +60,14 @@ struct TreeView {
   int32_t nv;
   int32_t depth;    // traversal stack bound (TNode levels)
   int32_t n_nodes;  // TNode count: no traversal visits more nodes than this
+  int32_t root;     // TNode where this tree's traversals start
 };
 
-// Host-side owner of one device tree.
+// Host-side owner of one device tree, or of a forest of independent trees
+// built together over consecutive row ranges (clouds) of one point array.
+// Tree positions, record ranges and leaf references are global over the
+// concatenated array; cloud c's points occupy positions
+// [valid_off[c], valid_off[c+1]) and its traversals start at root_tnode[c].
 struct TreeBase {
   int dtype = F32, dim = 3;
   int64_t n = 0, nv = 0;
@@ -69,10 +76,17 @@ struct TreeBase {
   double empty_split = 0.2;
   int device = 0;
   cudaStream_t stream = 0;  // allocations are stream-ordered on this stream
-  void* pts = nullptr;     // PointRec<T, D>[nv]
-  void* recs = nullptr;    // Rec<T, D>[n_recs]
-  void* tnodes = nullptr;  // TNode<T, D>[n_tnodes]
-  int32_t* fwd = nullptr;  // original index -> tree position, -1 if dropped
+  void* pts = nullptr;      // PointRec<T, D>[nv]
+  void* recs = nullptr;     // Rec<T, D>[n_recs]
+  void* tnodes = nullptr;   // TNode<T, D>[n_tnodes]
+  int32_t* fwd = nullptr;   // original index -> tree position, -1 if dropped
+  int ncloud = 1;
+  int32_t* root_rec = nullptr;    // device [ncloud]: root record per cloud (-1: no valid point)
+  int32_t* root_tnode = nullptr;  // device [ncloud]
+  int64_t* valid_off = nullptr;   // device [ncloud + 1]
+  int64_t* orig_off = nullptr;    // device [ncloud + 1]
+  std::vector<int32_t> root_tnode_h;
+  std::vector<int64_t> valid_off_h, orig_off_h;
   double root_lo[4] = {0, 0, 0, 0}, root_hi[4] = {0, 0, 0, 0};
   size_t device_bytes() const;
   ~TreeBase();
