@@ -166,6 +166,37 @@ PPTKG_API int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* 
                                          int num_eigen, int precision, void* out_evecs, void* out_evals,
                                          int32_t* out_sizes, void* stream);
 
+/* Forests (ragged batches).  Builds one tree per cloud over the consecutive
+ * row ranges [offsets[c], offsets[c+1]) of one point array (offsets: host,
+ * ncloud + 1 entries, offsets[0] = 0, offsets[ncloud] = n), each tree exactly
+ * the one pptkg_tree_build gives for that cloud alone; one build pass serves
+ * all clouds.  The reference builds such batches one KdTree per cloud
+ * (kdtree-impl.h:773-833).  The handle works with pptkg_tree_info,
+ * pptkg_tree_reverse_indices (global positions) and pptkg_tree_set_bucket. */
+PPTKG_API int pptkg_forest_build(const void* points, int64_t n, int dim, int dtype, int mem, const int64_t* offsets,
+                                 int ncloud, int max_leaf_size, double empty_split, void* stream, pptkg_tree** out);
+
+/* Number of clouds and (optionally, host, ncloud + 1) the first tree position
+ * of each cloud's valid points. */
+PPTKG_API int pptkg_forest_info(const pptkg_tree* forest, int* ncloud, int64_t* valid_offsets);
+
+/* Reference node list of one cloud's tree (layout of pptkg_tree_ref_nodes). */
+PPTKG_API int pptkg_forest_ref_nodes(const pptkg_tree* forest, int cloud, double* out, int64_t capacity,
+                                     int64_t* count);
+
+/* k nearest neighbours of every valid point among the points of its own
+ * cloud (optionally excluding itself, as KNearestNeighborsSelf does).  Outputs
+ * are indexed by global input row: out_idx n x k (global rows, -1 padded),
+ * out_cnt n; rows of dropped points get no neighbours. */
+PPTKG_API int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int exclude_self, int mem,
+                               int32_t* out_idx, int32_t* out_cnt, void* stream);
+
+/* PCA normals of every point over its cloud's k nearest neighbours (itself
+ * included, within r), the estimate_normals computation for all clouds at
+ * once; outputs indexed by global input row (layouts of pptkg_estimate_normals). */
+PPTKG_API int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
+                                   void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream);
+
 /* Batched symmetric 3x3 eigensolve of m row-major matrices of dtype F32/F64:
  * w m x 3 ascending; V m x 3 x 3 with layout 0: V[i, :, j] = j-th
  * eigenvector (vfuncs._eigh, pptk/vfuncs/vfuncs.cpp:1241-1293), layout 1:

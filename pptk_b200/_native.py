@@ -54,6 +54,14 @@ SIGNATURES = {
     "pptkg_estimate_normals": [_vp, _i64, _int, _int, _int, _flt, _vp, _i64, _int, _int, _vp, _vp, _vp, _vp],
     "pptkg_tree_normals": [_vp, _vp, _i64, _int, _int, _flt, _int, _int, _vp, _vp, _vp, _vp],
     "pptkg_eigh3": [_vp, _i64, _int, _int, _vp, _vp, _int, _vp],
+    "pptkg_forest_build": [_vp, _i64, _int, _int, _int, _vp, _int, _int, _dbl, _vp, _pvp],
+    "pptkg_forest_info": [_vp, _pint, _vp],
+    "pptkg_forest_ref_nodes": [_vp, _int, _vp, _i64, _pi64],
+    "pptkg_forest_knn": [_vp, _int, _dbl, _int, _int, _vp, _vp, _vp],
+    "pptkg_forest_normals": [_vp, _int, _flt, _int, _int, _int, _vp, _vp, _vp, _vp],
+    "pptkg_tree_normals_noalloc": [_vp, _vp, _i64, _int, _flt, _int, _int, _vp, _vp, _vp, _vp],
+    "pptkg_profile_enable": [_int],
+    "pptkg_profile_get": [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), _pi64],
 }
 
 _lib = None
@@ -78,6 +86,8 @@ def lib():
                     fn = getattr(handle, name)
                     fn.argtypes = args
                     fn.restype = ctypes.c_int
+                handle.pptkg_launch_count.argtypes = []
+                handle.pptkg_launch_count.restype = ctypes.c_int64
                 _lib = handle
     return _lib
 

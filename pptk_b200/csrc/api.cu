@@ -136,7 +136,7 @@ constexpr double DEFAULT_GAP = 1e-3;
 // record is preceded by its chain of empty-split nodes (kdtree-impl.h:
 // 114-158); a record without split or trims adds no node.
 template <typename T, int D>
-void serialize_nodes(const std::vector<Rec<T, D>>& recs, int r, std::vector<double>& out) {
+void serialize_nodes(const std::vector<Rec<T, D>>& recs, int r, int64_t base, std::vector<double>& out) {
   if (r < 0) return;
   const Rec<T, D>& rec = recs[r];
   const bool split = rec.split_dim >= 0;
@@ -145,7 +145,7 @@ void serialize_nodes(const std::vector<Rec<T, D>>& recs, int r, std::vector<doub
     const int dim = rec.trim[i] >> 1, side = rec.trim[i] & 1;
     const bool has_next = (i + 1 < nt) || split;
     out.push_back(dim);
-    out.push_back(side == 0 ? rec.begin : rec.end);
+    out.push_back((double)((side == 0 ? rec.begin : rec.end) - base));
     out.push_back(side == 0 ? (double)rec.lo[dim] : (double)rec.hi[dim]);
     out.push_back(side == 1 && has_next ? 1.0 : 0.0);
     out.push_back(side == 0 && has_next ? 1.0 : 0.0);
@@ -153,12 +153,12 @@ void serialize_nodes(const std::vector<Rec<T, D>>& recs, int r, std::vector<doub
   if (!split) return;
   auto emits = [&](int c) { return c >= 0 && (recs[c].split_dim >= 0 || recs[c].ntrim > 0); };
   out.push_back(rec.split_dim);
-  out.push_back(rec.split_index);
+  out.push_back((double)(rec.split_index - base));
   out.push_back((double)rec.split_val);
   out.push_back(emits(rec.left) ? 1.0 : 0.0);
   out.push_back(emits(rec.right) ? 1.0 : 0.0);
-  serialize_nodes<T, D>(recs, rec.left, out);
-  serialize_nodes<T, D>(recs, rec.right, out);
+  serialize_nodes<T, D>(recs, rec.left, base, out);
+  serialize_nodes<T, D>(recs, rec.right, base, out);
 }
 
 // Shared staging of an r-near query batch.
@@ -220,6 +220,8 @@ static void run_normals(const TreeBase* t, const int32_t* indices, int64_t m, in
 
 extern "C" {
 
+static int ref_nodes(const pptkg_tree* tree, int cloud, double* out, int64_t capacity, int64_t* count);
+
 int pptkg_version(void) { return 100; }
 
 int pptkg_last_error(char* buf, size_t len) {
@@ -246,6 +248,85 @@ int pptkg_tree_build(const void* points, int64_t n, int dim, int dtype, int mem,
       std::unique_ptr<pptkg_tree> h(new pptkg_tree());
       h->t.reset(build_tree<T, Dm>(in.d, n, max_leaf_size, empty_split, DEFAULT_BUCKET, S(stream)));
       *out = h.release();
+    });
+  });
+}
+
+int pptkg_forest_build(const void* points, int64_t n, int dim, int dtype, int mem, const int64_t* offsets,
+                       int ncloud, int max_leaf_size, double empty_split, void* stream, pptkg_tree** out) {
+  return guarded([&] {
+    if (!out) throw Error(E_INVALID, "out is null");
+    *out = nullptr;
+    if (n < 0) throw Error(E_INVALID, "negative point count");
+    if (n > 0 && !points) throw Error(E_INVALID, "points is null");
+    if (ncloud < 1 || !offsets) throw Error(E_INVALID, "need at least one cloud and its offsets");
+    if (!(empty_split >= 0.0)) throw Error(E_INVALID, "emptysplit must be non-negative");
+    dispatch_build(dtype, dim, [&](auto t, auto d) {
+      typedef decltype(t) T;
+      constexpr int Dm = decltype(d)::value;
+      Staged<T> in(points, (size_t)n * Dm, mem, true, S(stream));
+      std::unique_ptr<pptkg_tree> h(new pptkg_tree());
+      h->t.reset(build_forest<T, Dm>(in.d, n, offsets, ncloud, max_leaf_size, empty_split, DEFAULT_BUCKET, S(stream)));
+      *out = h.release();
+    });
+  });
+}
+
+int pptkg_forest_info(const pptkg_tree* forest, int* ncloud, int64_t* valid_offsets) {
+  return guarded([&] {
+    const TreeBase* t = tree_of(forest);
+    if (ncloud) *ncloud = t->ncloud;
+    if (valid_offsets) std::copy(t->valid_off_h.begin(), t->valid_off_h.end(), valid_offsets);
+  });
+}
+
+int pptkg_forest_ref_nodes(const pptkg_tree* forest, int cloud, double* out, int64_t capacity, int64_t* count) {
+  if (cloud < 0) {
+    g_msg = "cloud index out of range";
+    g_code = PPTKG_E_INVALID;
+    return g_code;
+  }
+  return ref_nodes(forest, cloud, out, capacity, count);
+}
+
+int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int exclude_self, int mem, int32_t* out_idx,
+                     int32_t* out_cnt, void* stream) {
+  return guarded([&] {
+    const TreeBase* t = tree_of(forest);
+    DeviceGuard g(t->device);
+    if (k < 1) throw Error(E_INVALID, "k must be positive");
+    if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
+    if (t->n && !out_idx) throw Error(E_INVALID, "out_idx is null");
+    dispatch_query(t, [&](auto tt, auto d) {
+      typedef decltype(tt) T;
+      constexpr int Dm = decltype(d)::value;
+      Staged<int32_t> oi(out_idx, (size_t)t->n * k, mem, false, S(stream));
+      Staged<int32_t> oc(out_cnt, (size_t)t->n, mem, false, S(stream));
+      forest_knn<T, Dm>(t, k, dmax, exclude_self != 0, oi.d, oc.d, S(stream));
+      oi.flush(S(stream));
+      oc.flush(S(stream));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+  });
+}
+
+int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
+                         void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream) {
+  return guarded([&] {
+    const TreeBase* t = tree_of(forest);
+    DeviceGuard g(t->device);
+    if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
+    if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
+    dispatch_float(t->dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      Staged<T> ev(out_evecs, (size_t)t->n * 3 * num_eigen, mem, false, S(stream));
+      Staged<T> ew(out_evals, (size_t)t->n * num_eigen, mem, false, S(stream));
+      Staged<int32_t> sz(out_sizes, (size_t)t->n, mem, false, S(stream));
+      forest_normals<T>(t, k, r, num_eigen, precision, DEFAULT_GAP, ev.d, ew.d, sz.d, S(stream));
+      ev.flush(S(stream));
+      ew.flush(S(stream));
+      sz.flush(S(stream));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
     });
   });
 }
@@ -301,7 +382,8 @@ static int ref_nodes(const pptkg_tree* tree, int cloud, double* out, int64_t cap
       int root = -1;
       PPTKG_CUDA(cudaMemcpy(&root, t->root_rec + (cloud < 0 ? 0 : cloud), sizeof(int), cudaMemcpyDeviceToHost));
       std::vector<double> v;
-      if (t->n_recs && root >= 0) serialize_nodes<T, Dm>(recs, root, v);
+      const int64_t base = t->valid_off_h.empty() ? 0 : t->valid_off_h[cloud < 0 ? 0 : cloud];
+      if (t->n_recs && root >= 0) serialize_nodes<T, Dm>(recs, root, base, v);
       const int64_t cnt = (int64_t)(v.size() / 5);
       if (count) *count = cnt;
       if (out) {

@@ -1126,6 +1126,8 @@ TreeBase::~TreeBase() {
   if (root_tnode) cudaFreeAsync(root_tnode, stream);
   if (valid_off) cudaFreeAsync(valid_off, stream);
   if (orig_off) cudaFreeAsync(orig_off, stream);
+  if (slot_off) cudaFreeAsync(slot_off, stream);
+  if (warp_cloud) cudaFreeAsync(warp_cloud, stream);
 }
 
 #define PPTKG_INST_BUILD(T, D)                                                                                  \

@@ -92,6 +92,25 @@ struct IndexQueries {
   }
 };
 
+// Forest queries: every valid point of every cloud, in tree order, each
+// cloud's range padded to whole warps so that a warp never mixes trees.
+struct SlotMap {
+  const int* warp_cloud;     // cloud of each warp; null outside forest mode
+  const int64_t* slot_off;   // first slot of each cloud
+  const int64_t* valid_off;  // first tree position of each cloud
+  const int* root_tnode;     // traversal root of each cloud
+};
+
+// Resolves the query of a slot: its output row (-1: padding) and, in forest
+// mode, the warp's tree root.
+template <typename T, int D>
+__device__ __forceinline__ int forest_query(int slot, const SlotMap& fm, TreeView<T, D>& tv) {
+  const int c = fm.warp_cloud[slot >> 5];
+  tv.root = fm.root_tnode[c];
+  const int64_t p = fm.valid_off[c] + (slot - fm.slot_off[c]);
+  return p < fm.valid_off[c + 1] ? tv.pts[p].id : -1;
+}
+
 // order_mode 0: slot = query; 1: order[slot]; 2: tree order (query = the
 // original index stored at tree position slot).
 template <typename T, int D>
@@ -198,7 +217,7 @@ int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaS
 template <typename T, int D, int KMAX, typename L>
 __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
                                                   int k, typename DistOf<T>::type r2, int32_t* out_idx,
-                                                  int32_t* out_cnt, int* status) {
+                                                  int32_t* out_cnt, int* status, SlotMap fm) {
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
@@ -206,7 +225,10 @@ __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const
   int qid = -1, own = -1;
   DistT q[D];
   bool active = false;
-  if (slot < m) {
+  if (fm.warp_cloud) {
+    qid = forest_query(slot, fm, tv);
+    if (qid >= 0) active = ld.load(qid, tv, q, own);
+  } else if (slot < m) {
     qid = query_of(slot, order, order_mode, tv);
     active = ld.load(qid, tv, q, own);
   }
@@ -216,7 +238,7 @@ __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
   if (!packet_knn<T, D>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
-  if (slot < m) {
+  if (qid >= 0) {
     int c = 0;
 #pragma unroll
     for (int j = 0; j < KMAX; j++) {
@@ -232,28 +254,29 @@ __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const
 
 template <typename T, int D, int KMAX, typename L>
 void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
-                int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st) {
+                int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm) {
+  if (m <= 0) return;
   const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
   if (smem > 48 * 1024)
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
-                                                                      d_idx, d_cnt, status);
+                                                                      d_idx, d_cnt, status, fm);
   PPTKG_CHECK_LAUNCH();
 }
 
 template <typename T, int D, typename L>
 void dispatch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
-                  int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st) {
+                  int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (k <= 4)
-    launch_knn<T, D, 4>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+    launch_knn<T, D, 4>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
   else if (k <= 8)
-    launch_knn<T, D, 8>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+    launch_knn<T, D, 8>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
   else if (k <= 16)
-    launch_knn<T, D, 16>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+    launch_knn<T, D, 16>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
   else if (k <= 32)
-    launch_knn<T, D, 32>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+    launch_knn<T, D, 32>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
   else
-    launch_knn<T, D, 64>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st);
+    launch_knn<T, D, 64>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
 }
 
 template <typename DistT>
@@ -520,7 +543,7 @@ __global__ void __launch_bounds__(QTHREADS, normals_min_blocks(KMAX, sizeof(type
 k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
-                                                      int* fix, int* nfix, int* status) {
+                                                      int* fix, int* nfix, int* status, SlotMap fm) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
@@ -530,7 +553,10 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   int qid = -1, own = -1;
   DistT q[3];
   bool active = false;
-  if (slot < m) {
+  if (fm.warp_cloud) {
+    qid = forest_query(slot, fm, tv);
+    if (qid >= 0) active = ld.load(qid, tv, q, own);
+  } else if (slot < m) {
     qid = query_of(slot, order, order_mode, tv);
     active = ld.load(qid, tv, q, own);
   }
@@ -539,7 +565,7 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
   if (!packet_knn<T, 3>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
-  if (slot >= m) return;
+  if (qid < 0) return;
   if (!active) {
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
     return;
@@ -668,30 +694,31 @@ __global__ void k_refine64(const PointRec<T, 3>* pts, const int* fwd, const int*
 template <typename T, int KMAX, typename L, int PREC>
 void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
-                    cudaStream_t st) {
+                    cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (m <= 0) return;
   const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
-      view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status);
+      view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm);
   PPTKG_CHECK_LAUNCH();
 }
 
 template <typename T, int KMAX, typename L>
 void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
-                  int num_eigen, int prec, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st) {
+                  int num_eigen, int prec, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st,
+                  SlotMap fm = SlotMap{}) {
   if (prec == PREC_FP64) {
     launch_normals<T, KMAX, L, PREC_FP64>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, nullptr,
-                                          nullptr, status, st);
+                                          nullptr, status, st, fm);
     return;
   }
   // FP32 pass, then an FP64 re-solve of the queued small-gap neighbourhoods
   DevBuf<int> fix((size_t)std::max(m, 1) * (KMAX + 2), st), nfix(1, st);
   PPTKG_CUDA(cudaMemsetAsync(nfix.get(), 0, sizeof(int), st));
   launch_normals<T, KMAX, L, PREC_FP32>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix.get(),
-                                        nfix.get(), status, st);
+                                        nfix.get(), status, st, fm);
   {
     Stage s("normals.refine64", st);
     k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, t->fwd, fix.get(), nfix.get(),
@@ -703,17 +730,17 @@ void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, in
 template <typename T, typename L>
 void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k,
                       typename DistOf<T>::type r2, int num_eigen, int prec, double gap_thr, T* ev, T* ew,
-                      int32_t* sz, int* status, cudaStream_t st) {
+                      int32_t* sz, int* status, cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (k <= 4)
-    normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
   else if (k <= 8)
-    normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
   else if (k <= 16)
-    normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
   else if (k <= 32)
-    normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
   else
-    normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st);
+    normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
 }
 
 template <typename T>
@@ -786,6 +813,112 @@ void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStre
   k_eigh3<T><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(d_A, m, d_w, d_V, layout);
   PPTKG_CHECK_LAUNCH();
 }
+
+// ------------------------------------------------------------ forests ----
+__global__ void k_warp_cloud(const int64_t* slot_off, int ncloud, int64_t nwarps, int* warp_cloud) {
+  const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwarps) return;
+  const int64_t s = w * 32;
+  int lo = 0, hi = ncloud - 1;  // last cloud whose first slot is <= s
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (slot_off[mid] <= s)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  warp_cloud[w] = lo;
+}
+
+// Slot map of a forest (cached on the tree): cloud c's valid points take the
+// slots [slot_off[c], slot_off[c] + count), rounded up to whole warps.
+static SlotMap slot_map(const TreeBase* t, int64_t& n_slots, cudaStream_t st) {
+  TreeBase* mt = const_cast<TreeBase*>(t);
+  if (!mt->warp_cloud) {
+    std::vector<int64_t> so(t->ncloud + 1, 0);
+    for (int c = 0; c < t->ncloud; c++) {
+      const int64_t cnt = t->valid_off_h[c + 1] - t->valid_off_h[c];
+      so[c + 1] = so[c] + (cnt + 31) / 32 * 32;
+    }
+    mt->n_slots = so[t->ncloud];
+    if (mt->n_slots > INT32_MAX) throw Error(E_INVALID, "forest too large for one query pass");
+    PPTKG_CUDA(cudaMallocAsync((void**)&mt->slot_off, sizeof(int64_t) * (t->ncloud + 1), st));
+    PPTKG_CUDA(cudaMemcpyAsync(mt->slot_off, so.data(), sizeof(int64_t) * (t->ncloud + 1), cudaMemcpyHostToDevice, st));
+    const int64_t nw = std::max<int64_t>(mt->n_slots / 32, 1);
+    PPTKG_CUDA(cudaMallocAsync((void**)&mt->warp_cloud, sizeof(int) * nw, st));
+    if (mt->n_slots > 0) {
+      k_warp_cloud<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(mt->slot_off, t->ncloud, nw, mt->warp_cloud);
+      PPTKG_CHECK_LAUNCH();
+    }
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+  }
+  n_slots = mt->n_slots;
+  return SlotMap{mt->warp_cloud, mt->slot_off, t->valid_off, t->root_tnode};
+}
+
+template <typename T, int D>
+void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_t* d_idx, int32_t* d_cnt,
+                cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k < 1) throw Error(E_INVALID, "k must be positive");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU kNN kernels");
+  int64_t n_slots = 0;
+  const SlotMap fm = slot_map(t, n_slots, st);
+  // rows of dropped (NaN/inf) points are not visited: no neighbours
+  PPTKG_CUDA(cudaMemsetAsync(d_idx, 0xff, sizeof(int32_t) * (size_t)t->n * k, st));
+  if (d_cnt) PPTKG_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)t->n, st));
+  if (n_slots == 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  const DistT r2 = radius2<DistT>(dmax);
+  Stage stage("forest.knn", st);
+  if (exclude_self)
+    dispatch_knn<T, D>(t, IndexQueries<D, true>{nullptr, t->fwd}, nullptr, 0, (int)n_slots, k, r2, d_idx, d_cnt,
+                       status.get(), st, fm);
+  else
+    dispatch_knn<T, D>(t, IndexQueries<D, false>{nullptr, t->fwd}, nullptr, 0, (int)n_slots, k, r2, d_idx, d_cnt,
+                       status.get(), st, fm);
+  check_status(status.get(), st, "forest knn");
+}
+
+template <typename T>
+__global__ void k_fill_invalid(int64_t n, int num_eigen, T* evecs, T* evals, int32_t* sizes) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) write_invalid<T>((int)i, num_eigen, evecs, evals, sizes);
+}
+
+template <typename T>
+void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
+                    T* d_evals, int32_t* d_sizes, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+  if (k < 1) throw Error(E_INVALID, "forest normals need k >= 1");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU normal kernels");
+  int64_t n_slots = 0;
+  const SlotMap fm = slot_map(t, n_slots, st);
+  if (t->n > t->nv && t->n > 0) {
+    k_fill_invalid<T><<<(unsigned)((t->n + 255) / 256), 256, 0, st>>>(t->n, num_eigen, d_evecs, d_evals, d_sizes);
+    PPTKG_CHECK_LAUNCH();
+  }
+  if (n_slots == 0) return;
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  const DistT rr = (DistT)(T)r;
+  const DistT r2 = rr * rr;
+  int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
+  Stage stage("forest.normals", st);
+  dispatch_normals<T, IndexQueries<3, false>>(t, IndexQueries<3, false>{nullptr, t->fwd}, nullptr, 0, (int)n_slots,
+                                              k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals, d_sizes, status.get(),
+                                              st, fm);
+  check_status(status.get(), st, "forest normals");
+}
+
+template void forest_knn<float, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
+template void forest_knn<double, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
+template void forest_normals<float>(const TreeBase*, int, float, int, int, double, float*, float*, int32_t*,
+                                    cudaStream_t);
+template void forest_normals<double>(const TreeBase*, int, float, int, int, double, double*, double*, int32_t*,
+                                     cudaStream_t);
 
 // ------------------------------------------- allocation-free normals ----
 // Scratch of pptkg_tree_normals_noalloc, resident on every GPU that loads the

@@ -41,6 +41,15 @@ template <typename T>
 void normals_query(const TreeBase* t, const QuerySpec& qs, int k, float r, int num_eigen, int precision,
                    double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st);
 
+// Queries over every valid point of every cloud of a forest, each against
+// its own cloud's tree; outputs are indexed by global input row (n rows).
+template <typename T, int D>
+void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_t* d_idx, int32_t* d_cnt,
+                cudaStream_t st);
+template <typename T>
+void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
+                    T* d_evals, int32_t* d_sizes, cudaStream_t st);
+
 // pptkg_tree_normals_noalloc: the tree-normals path with its scratch in a
 // static device array instead of allocated memory (device pointers only).
 template <typename T>

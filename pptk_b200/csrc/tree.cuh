@@ -86,6 +86,9 @@ struct TreeBase {
   int64_t* valid_off = nullptr;   // device [ncloud + 1]
   int64_t* orig_off = nullptr;    // device [ncloud + 1]
   std::vector<int32_t> root_tnode_h;
+  int64_t n_slots = 0;             // forest query slots (cached slot map)
+  int64_t* slot_off = nullptr;     // device [ncloud + 1]
+  int32_t* warp_cloud = nullptr;   // device [n_slots / 32]
   std::vector<int64_t> valid_off_h, orig_off_h;
   double root_lo[4] = {0, 0, 0, 0}, root_hi[4] = {0, 0, 0, 0};
   size_t device_bytes() const;

@@ -1,0 +1,120 @@
+"""Ragged batches: thousands of independent clouds built and queried together.
+
+A ``Forest`` holds one k-d tree per cloud of a CSR batch (points concatenated,
+``offsets[c]:offsets[c+1]`` the rows of cloud c).  Each tree is exactly the
+tree ``pptk.kdtree._build`` gives for that cloud alone, but all clouds are
+built in one device build pass and queried in one launch: warps are assigned
+to clouds, each cloud's queries padded to whole warps, and every warp walks
+its own cloud's tree.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _native as N
+
+_CODES = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}
+
+
+class Forest:
+    """Device-resident trees of a ragged batch of clouds."""
+
+    def __init__(self, points, offsets, maxleafsize=10, emptysplit=0.2):
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.int64))
+        if off.ndim != 1 or off.size < 2:
+            raise ValueError("offsets must hold at least two entries")
+        if N.is_torch_cuda(points):
+            import torch
+            if points.dtype not in (torch.float32, torch.float64):
+                raise TypeError("points must be float32 or float64")
+            p = points.contiguous()
+            code = 0 if p.dtype == torch.float32 else 1
+            mem, self._stream, self.device = N.MEM_DEVICE, N.torch_stream(p.device), p.device
+        else:
+            p = np.ascontiguousarray(points)
+            if p.dtype not in _CODES:
+                raise TypeError("points must be float32 or float64")
+            code = _CODES[p.dtype]
+            mem, self._stream, self.device = N.MEM_HOST, None, None
+        if p.ndim != 2 or p.shape[1] not in (2, 3, 4):
+            raise ValueError("points must be (n, 2..4)")
+        if off[0] != 0 or off[-1] != p.shape[0] or (np.diff(off) < 0).any():
+            raise ValueError("offsets must start at 0, end at n and not decrease")
+        self.n, self.dim = int(p.shape[0]), int(p.shape[1])
+        self.dtype = np.dtype(np.float32) if code == 0 else np.dtype(np.float64)
+        self.offsets = off
+        self.ncloud = off.size - 1
+        self._h = ctypes.c_void_p()
+        N.call("pptkg_forest_build", N.ptr(p), self.n, self.dim, code, mem, N.ptr(off), self.ncloud, int(maxleafsize),
+               float(emptysplit), self._stream, ctypes.byref(self._h), where="Forest()")
+        vo = np.empty(self.ncloud + 1, np.int64)
+        nc = ctypes.c_int()
+        N.call("pptkg_forest_info", self._h, ctypes.byref(nc), N.ptr(vo))
+        self.valid_offsets = vo
+        self.n_valid = int(vo[-1])
+        self._torch = mem == N.MEM_DEVICE
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                N.lib().pptkg_tree_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _new(self, shape, dtype):
+        if self._torch:
+            import torch
+            tdt = {np.dtype(np.int32): torch.int32, np.dtype(np.float32): torch.float32,
+                   np.dtype(np.float64): torch.float64}[np.dtype(dtype)]
+            return torch.empty(shape, dtype=tdt, device=self.device)
+        return np.empty(shape, dtype)
+
+    @property
+    def _mem(self):
+        return N.MEM_DEVICE if self._torch else N.MEM_HOST
+
+    def reverse_indices(self):
+        """Global tree position -> global input row."""
+        out = np.empty(self.n_valid, np.int32)
+        N.call("pptkg_tree_reverse_indices", self._h, N.ptr(out), N.MEM_HOST, None)
+        return out
+
+    def ref_nodes(self, cloud):
+        """Reference node list of one cloud's tree (preorder, 5 columns)."""
+        cnt = ctypes.c_int64()
+        N.call("pptkg_forest_ref_nodes", self._h, int(cloud), None, 0, ctypes.byref(cnt))
+        out = np.empty((cnt.value, 5), np.float64)
+        N.call("pptkg_forest_ref_nodes", self._h, int(cloud), N.ptr(out), cnt.value, ctypes.byref(cnt))
+        return out
+
+    def set_bucket(self, bucket):
+        N.call("pptkg_tree_set_bucket", self._h, int(bucket), self._stream)
+
+    def knn(self, k, dmax=math.inf, exclude_self=True):
+        """k nearest neighbours of every point within its own cloud:
+        (indices n x k as global rows, -1 padded; counts n)."""
+        idx = self._new((self.n, int(k)), np.int32)
+        cnt = self._new((self.n,), np.int32)
+        N.call("pptkg_forest_knn", self._h, int(k), float(np.float32(dmax)), int(bool(exclude_self)), self._mem,
+               N.ptr(idx), N.ptr(cnt), self._stream, where="Forest.knn()")
+        return idx, cnt
+
+    def normals(self, k, r=math.inf, output_eigenvalues=False, output_all_eigenvectors=False,
+                output_neighborhood_sizes=False, precision="auto"):
+        """estimate_normals over every cloud at once (same layouts)."""
+        from .estimate_normals import PRECISIONS
+        if self.dim != 3:
+            raise TypeError("normals need 3-d points")
+        ne = 3 if output_all_eigenvectors else 1
+        ev = self._new((self.n, 3) if ne == 1 else (self.n, 3, 3), self.dtype)
+        ew = self._new((self.n,) if ne == 1 else (self.n, 3), self.dtype) if output_eigenvalues else None
+        sz = self._new((self.n,), np.int32) if output_neighborhood_sizes else None
+        N.call("pptkg_forest_normals", self._h, int(k), ctypes.c_float(float(np.float32(r))), ne,
+               PRECISIONS[precision], self._mem, N.ptr(ev), N.ptr(ew), N.ptr(sz), self._stream,
+               where="Forest.normals()")
+        if ew is None and sz is None:
+            return ev
+        return ev, ew, sz

@@ -1,0 +1,85 @@
+"""Ragged batches (forests) on the GPU: every cloud's tree is the reference
+tree for that cloud alone, and one forest query equals per-cloud queries."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch(seed=0, count=40, dtype=np.float32):
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(1, 3000, count)
+    sizes[3] = 0          # an empty cloud
+    sizes[5] = 7          # smaller than a leaf
+    sizes[7] = 9000       # above the per-CTA subtree size
+    clouds = [rng.normal(size=(s, 3)).astype(dtype) * rng.uniform(0.1, 5.0) for s in sizes]
+    clouds[9][::13] = np.nan  # dropped rows
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    return np.concatenate(clouds), off, clouds
+
+
+def test_forest_trees_are_the_reference_trees(gpu, port):
+    from pptk_b200 import ragged
+    P, off, clouds = small_batch()
+    f = ragged.Forest(P, off)
+    assert f.ncloud == len(clouds)
+    rev = f.reverse_indices()
+    for c, cl in enumerate(clouds):
+        t = port.PortTree(cl)
+        lo, hi = f.valid_offsets[c], f.valid_offsets[c + 1]
+        assert np.array_equal(rev[lo:hi] - off[c], t.reverse_indices()), c
+        assert np.array_equal(f.ref_nodes(c), t.nodes()), c
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_forest_queries_equal_per_cloud_queries(gpu, port, dtype):
+    from pptk_b200 import ragged
+    P, off, clouds = small_batch(seed=1, dtype=dtype)
+    f = ragged.Forest(P, off)
+    idx, cnt = f.knn(8)
+    ev, ew, sz = f.normals(8, output_eigenvalues=True, output_neighborhood_sizes=True)
+    for c, cl in enumerate(clouds):
+        rows = slice(off[c], off[c + 1])
+        if len(cl) == 0:
+            continue
+        t = port.PortTree(cl)
+        nv = t.num_valid
+        oi, oc = t.knn_self(np.arange(len(cl), dtype=np.int32), 8)
+        gi = np.where(idx[rows] >= 0, idx[rows] - off[c], -1)
+        assert np.array_equal(cnt[rows], oc) and np.array_equal(gi, oi), c
+        # normals of the cloud alone through the drop-in API
+        z = gpu.estimate_normals(cl, 8, np.inf, output_eigenvalues=True, output_neighborhood_sizes=True,
+                                 verbose=False)
+        assert np.array_equal(sz[rows], z[2]), c
+        ok = np.isfinite(z[1])
+        dots = np.abs((ev[rows][ok].astype(np.float64) * z[0][ok]).sum(1))
+        assert (dots > 1 - 1e-6).all(), c
+        assert nv == int((z[2] > 0).sum())
+
+
+def test_forest_from_device_tensors(gpu):
+    import torch
+    from pptk_b200 import ragged
+    P, off, clouds = small_batch(seed=2, count=12)
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    idx, cnt = f.knn(4)
+    assert idx.is_cuda
+    g = ragged.Forest(P, off)
+    gi, gc = g.knn(4)
+    assert np.array_equal(idx.cpu().numpy(), gi) and np.array_equal(cnt.cpu().numpy(), gc)
+
+
+def test_ragged_config_shape_at_scale(gpu, port):
+    # 256 clouds of the config-4 shape (log-uniform sizes, blobs + plane);
+    # exact on sampled clouds, properties everywhere
+    from pptk_b200 import ragged, synth
+    P, off = synth.ragged_clouds(256, seed=4)
+    f = ragged.Forest(P, off)
+    idx, cnt = f.knn(16)
+    assert (cnt == np.minimum(16, np.diff(off).repeat(np.diff(off)) - 1)).all()
+    cloud_of = np.repeat(np.arange(256), np.diff(off))
+    assert (cloud_of[idx[:, 0]] == cloud_of).all()  # neighbours stay in their cloud
+    for c in (0, 17, 100, 255):
+        cl = P[off[c]:off[c + 1]]
+        oi, oc = port.PortTree(cl).knn_self(np.arange(len(cl), dtype=np.int32), 16)
+        assert np.array_equal(idx[off[c]:off[c + 1]] - off[c], oi)
