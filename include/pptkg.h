@@ -197,6 +197,19 @@ PPTKG_API int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int
 PPTKG_API int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
                                    void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream);
 
+/* Multi-tree batches (no reference counterpart; the serving loop's batching
+ * step).  One launch answers queries for several resident single trees:
+ * tree g answers the concatenated query rows [row_offsets[g],
+ * row_offsets[g+1]) (row_offsets: host, ntrees + 1 entries).  All trees
+ * share dtype and dim.  Results are exactly those of pptkg_knn /
+ * pptkg_tree_normals on each tree alone. */
+PPTKG_API int pptkg_multi_knn(const pptkg_tree* const* trees, int ntrees, const void* queries,
+                              const int64_t* row_offsets, int qdtype, int mem, int k, double dmax, int32_t* out_idx,
+                              int32_t* out_cnt, void* stream);
+PPTKG_API int pptkg_multi_normals(const pptkg_tree* const* trees, int ntrees, const int32_t* indices,
+                                  const int64_t* row_offsets, int mem, int k, float r, int num_eigen, int precision,
+                                  void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream);
+
 /* Batched symmetric 3x3 eigensolve of m row-major matrices of dtype F32/F64:
  * w m x 3 ascending; V m x 3 x 3 with layout 0: V[i, :, j] = j-th
  * eigenvector (vfuncs._eigh, pptk/vfuncs/vfuncs.cpp:1241-1293), layout 1:

@@ -331,6 +331,75 @@ int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen
   });
 }
 
+static std::vector<const TreeBase*> tree_list(const pptkg_tree* const* trees, int ntrees) {
+  if (ntrees < 1 || !trees) throw Error(E_INVALID, "need at least one tree");
+  std::vector<const TreeBase*> v(ntrees);
+  for (int g = 0; g < ntrees; g++) v[g] = tree_of(trees[g]);
+  for (int g = 1; g < ntrees; g++)
+    if (v[g]->device != v[0]->device) throw Error(E_INVALID, "all trees of a batch must live on one device");
+  return v;
+}
+
+int pptkg_multi_knn(const pptkg_tree* const* trees, int ntrees, const void* queries, const int64_t* row_offsets,
+                    int qdtype, int mem, int k, double dmax, int32_t* out_idx, int32_t* out_cnt, void* stream) {
+  return guarded([&] {
+    std::vector<const TreeBase*> v = tree_list(trees, ntrees);
+    DeviceGuard g(v[0]->device);
+    if (!row_offsets || row_offsets[0] != 0) throw Error(E_INVALID, "row offsets must start at 0");
+    const int64_t m = row_offsets[ntrees];
+    if (k < 1) throw Error(E_INVALID, "k must be positive");
+    if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
+    if (qdtype != F32 && qdtype != F64) throw Error(E_TYPE, "query points must be float32 or float64");
+    if (m && (!queries || !out_idx)) throw Error(E_INVALID, "null array");
+    dispatch_query(v[0], [&](auto tt, auto d) {
+      typedef decltype(tt) T;
+      constexpr int Dm = decltype(d)::value;
+      const size_t bytes = (size_t)m * Dm * dtype_size(qdtype);
+      DevBuf<char> qbuf;
+      const void* qd = queries;
+      if (mem == PPTKG_MEM_HOST && m) {
+        qbuf.alloc(bytes, S(stream));
+        PPTKG_CUDA(cudaMemcpyAsync(qbuf.get(), queries, bytes, cudaMemcpyDefault, S(stream)));
+        qd = qbuf.get();
+      }
+      Staged<int32_t> oi(out_idx, (size_t)m * k, mem, false, S(stream));
+      Staged<int32_t> oc(out_cnt, (size_t)m, mem, false, S(stream));
+      multi_knn<T, Dm>(v.data(), ntrees, qd, qdtype, row_offsets, k, dmax, oi.d, oc.d, S(stream));
+      oi.flush(S(stream));
+      oc.flush(S(stream));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+  });
+}
+
+int pptkg_multi_normals(const pptkg_tree* const* trees, int ntrees, const int32_t* indices,
+                        const int64_t* row_offsets, int mem, int k, float r, int num_eigen, int precision,
+                        void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream) {
+  return guarded([&] {
+    std::vector<const TreeBase*> v = tree_list(trees, ntrees);
+    DeviceGuard g(v[0]->device);
+    if (!row_offsets || row_offsets[0] != 0) throw Error(E_INVALID, "row offsets must start at 0");
+    const int64_t m = row_offsets[ntrees];
+    if (v[0]->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+    if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
+    if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
+    if (m && !indices) throw Error(E_INVALID, "indices is null");
+    dispatch_float(v[0]->dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      Staged<int32_t> qi(indices, (size_t)m, mem, true, S(stream));
+      Staged<T> ev(out_evecs, (size_t)m * 3 * num_eigen, mem, false, S(stream));
+      Staged<T> ew(out_evals, (size_t)m * num_eigen, mem, false, S(stream));
+      Staged<int32_t> sz(out_sizes, (size_t)m, mem, false, S(stream));
+      multi_normals<T>(v.data(), ntrees, qi.d, row_offsets, k, r, num_eigen, precision, DEFAULT_GAP, ev.d, ew.d,
+                       sz.d, S(stream));
+      ev.flush(S(stream));
+      ew.flush(S(stream));
+      sz.flush(S(stream));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+  });
+}
+
 int pptkg_tree_free(pptkg_tree* tree) {
   return guarded([&] { delete tree; });
 }

@@ -1,6 +1,7 @@
 // Query kernels: exact kNN (point and self forms), r-near count/fill in the
 // reference's order, and fused kNN + PCA normal estimation.
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -24,6 +25,7 @@ TreeView<T, D> view_of(const TreeBase* t) {
   v.depth = t->tdepth;
   v.n_nodes = t->n_tnodes;
   v.root = t->root_tnode_h.empty() ? 0 : t->root_tnode_h[0];
+  v.fwd = t->fwd;
   return v;
 }
 
@@ -81,7 +83,7 @@ struct IndexQueries {
   template <typename T, typename DistT>
   __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own) const {
     const int o = idx ? idx[i] : i;
-    const int p = fwd[o];
+    const int p = (fwd ? fwd : tv.fwd)[o];
     own = -1;
     if (p < 0) return false;  // the point was dropped (NaN/inf): no neighbours
     const PointRec<T, D> r = tv.pts[p];
@@ -94,18 +96,31 @@ struct IndexQueries {
 
 // Forest queries: every valid point of every cloud, in tree order, each
 // cloud's range padded to whole warps so that a warp never mixes trees.
+//
+// Multi-tree batches (`views` set): group g is a separate tree with its own
+// TreeView; its query rows [row_off[g], row_off[g+1]) take the slots from
+// slot_off[g], rounded up to whole warps.
 struct SlotMap {
-  const int* warp_cloud;     // cloud of each warp; null outside forest mode
-  const int64_t* slot_off;   // first slot of each cloud
-  const int64_t* valid_off;  // first tree position of each cloud
-  const int* root_tnode;     // traversal root of each cloud
+  const int* warp_cloud;     // group (cloud or tree) of each warp; null: plain mode
+  const int64_t* slot_off;   // first slot of each group
+  const int64_t* valid_off;  // forest: first tree position of each cloud
+  const int* root_tnode;     // forest: traversal root of each cloud
+  const void* views;         // multi-tree: TreeView<T, D> per group
+  const int64_t* row_off;    // multi-tree: first query row per group
+  const int* order;          // multi-tree: query row of each batch position (null: identity)
 };
 
-// Resolves the query of a slot: its output row (-1: padding) and, in forest
-// mode, the warp's tree root.
+// Resolves the query of a slot: its output row (-1: padding) and the warp's
+// tree (root, or the whole view in multi-tree mode).
 template <typename T, int D>
 __device__ __forceinline__ int forest_query(int slot, const SlotMap& fm, TreeView<T, D>& tv) {
   const int c = fm.warp_cloud[slot >> 5];
+  if (fm.views) {
+    tv = static_cast<const TreeView<T, D>*>(fm.views)[c];
+    const int64_t row = fm.row_off[c] + (slot - fm.slot_off[c]);
+    if (row >= fm.row_off[c + 1]) return -1;
+    return fm.order ? fm.order[row] : (int)row;
+  }
   tv.root = fm.root_tnode[c];
   const int64_t p = fm.valid_off[c] + (slot - fm.slot_off[c]);
   return p < fm.valid_off[c + 1] ? tv.pts[p].id : -1;
@@ -185,8 +200,8 @@ __global__ void k_place(const int* key, int m, int* cursor, int* order) {
 // Builds a processing order in which queries near each other in the tree are
 // adjacent (counting sort on the tree position key).  Returns the order mode.
 template <typename T, int D>
-int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaStream_t st) {
-  check_indices(t, qs, st);
+int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaStream_t st, bool checked = false) {
+  if (!checked) check_indices(t, qs, st);
   Stage stage("order", st);
   const int m = (int)qs.m;
   const int nv = (int)t->nv;
@@ -550,10 +565,11 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   if ((slot & ~31) >= m) return;
   WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
   const int lane = threadIdx.x & 31;
-  int qid = -1, own = -1;
+  int qid = -1, own = -1, grp = 0;
   DistT q[3];
   bool active = false;
   if (fm.warp_cloud) {
+    grp = fm.views ? fm.warp_cloud[slot >> 5] : 0;
     qid = forest_query(slot, fm, tv);
     if (qid >= 0) active = ld.load(qid, tv, q, own);
   } else if (slot < m) {
@@ -584,11 +600,11 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
     float w[3], V[9];
     eigh3<float>(C, w, V);
     write_pca<T, float>(qid, n, w, V, num_eigen, evecs, evals, sizes);
-    if (fix && !(rel_gap<float>(w) >= (float)gap_thr)) {
+    if (fix && n > 0 && !(rel_gap<float>(w) >= (float)gap_thr)) {
       // queue [query, count, neighbour positions] for the FP64 re-solve
       int* e = fix + (int64_t)atomicAdd(nfix, 1) * (KMAX + 2);
       e[0] = qid;
-      e[1] = n;
+      e[1] = n | (grp << 8);
       for (int j = 0; j < n; j++) e[2 + j] = lane_log[j * 32];
     }
   }
@@ -650,16 +666,23 @@ __global__ void __launch_bounds__(QTHREADS) k_normals_rnear(TreeView<T, 3> tv, L
 }
 
 // FP64 re-solve of queued neighbourhoods: one thread per entry, a gather of
-// the stored neighbour positions, float64 covariance (shifted to the query
-// point, centred) and eigensolve; overwrites the FP32 results of that row.
+// the stored neighbour positions, float64 covariance (shifted to the first
+// neighbour, centred) and eigensolve; overwrites the FP32 results of that
+// output row.
+//
+// Entry layout: [output row, count | group << 8, positions...] with
+// 1 <= count <= KMAX; in a multi-tree batch the group selects the tree whose
+// points the positions refer to (views[group]), otherwise `pts` is the
+// tree's own.
 template <typename T, int KMAX>
-__global__ void k_refine64(const PointRec<T, 3>* pts, const int* fwd, const int* fix, const int* nfix, int num_eigen,
-                           T* evecs, T* evals, int32_t* sizes) {
+__global__ void k_refine64(const PointRec<T, 3>* pts, const int* fix, const int* nfix, int num_eigen, T* evecs,
+                           T* evals, int32_t* sizes, const TreeView<T, 3>* views) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= *nfix) return;
   const int* e = fix + (int64_t)i * (KMAX + 2);
-  const int qid = e[0], n = e[1];
-  const PointRec<T, 3> qr = pts[fwd[qid]];
+  const int qid = e[0], n = e[1] & 0xff, grp = e[1] >> 8;
+  if (views) pts = views[grp].pts;
+  const PointRec<T, 3> qr = pts[e[2]];
   double s0 = 0, s1 = 0, s2 = 0;
   for (int j = 0; j < n; j++) {
     const PointRec<T, 3> r = pts[e[2 + j]];
@@ -721,8 +744,9 @@ void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, in
                                         nfix.get(), status, st, fm);
   {
     Stage s("normals.refine64", st);
-    k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, t->fwd, fix.get(), nfix.get(),
-                                                        num_eigen, ev, ew, sz);
+    k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, fix.get(), nfix.get(),
+                                                        num_eigen, ev, ew, sz,
+                                                        static_cast<const TreeView<T, 3>*>(fm.views));
     PPTKG_CHECK_LAUNCH();
   }
 }
@@ -853,7 +877,7 @@ static SlotMap slot_map(const TreeBase* t, int64_t& n_slots, cudaStream_t st) {
     PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   n_slots = mt->n_slots;
-  return SlotMap{mt->warp_cloud, mt->slot_off, t->valid_off, t->root_tnode};
+  return SlotMap{mt->warp_cloud, mt->slot_off, t->valid_off, t->root_tnode, nullptr, nullptr, nullptr};
 }
 
 template <typename T, int D>
@@ -920,6 +944,186 @@ template void forest_normals<float>(const TreeBase*, int, float, int, int, doubl
 template void forest_normals<double>(const TreeBase*, int, float, int, int, double, double*, double*, int32_t*,
                                      cudaStream_t);
 
+// ---------------------------------------------------- multi-tree batches --
+// Device tables of a multi-tree batch: TreeViews, per-warp group, slot and
+// row offsets.  `rows` are host offsets (ntrees + 1) of each tree's queries.
+template <typename T, int D>
+struct MultiTables {
+  DevBuf<TreeView<T, D>> views;
+  DevBuf<int64_t> slot_off, row_off;
+  DevBuf<int> warp_tree, order;
+  bool ordered = false;
+  int64_t n_slots = 0;
+  int depth = 0, n_nodes = 0;
+  SlotMap map() const {
+    return SlotMap{warp_tree.get(), slot_off.get(), nullptr, nullptr, views.get(), row_off.get(),
+                   ordered ? order.get() : nullptr};
+  }
+};
+
+template <typename T, int D>
+void multi_tables(const TreeBase* const* trees, int ntrees, const int64_t* rows, MultiTables<T, D>& mt, cudaStream_t st) {
+  std::vector<TreeView<T, D>> v(ntrees);
+  std::vector<int64_t> so(ntrees + 1, 0);
+  for (int g = 0; g < ntrees; g++) {
+    const TreeBase* t = trees[g];
+    if (t->dtype != (sizeof(T) == 4 ? F32 : F64) || t->dim != D)
+      throw Error(E_TYPE, "all trees of a batch must share dtype and dim");
+    if (t->ncloud != 1) throw Error(E_INVALID, "multi-tree batches take single trees, not forests");
+    v[g] = view_of<T, D>(t);
+    mt.depth = std::max(mt.depth, t->tdepth);
+    mt.n_nodes = std::max(mt.n_nodes, t->n_tnodes);
+    const int64_t m = rows[g + 1] - rows[g];
+    if (m < 0) throw Error(E_INVALID, "query offsets must not decrease");
+    so[g + 1] = so[g] + (m + 31) / 32 * 32;
+  }
+  mt.n_slots = so[ntrees];
+  if (mt.n_slots > INT32_MAX) throw Error(E_INVALID, "batch too large for one pass");
+  // every view uses the batch-wide stack bound (shared memory is sized once)
+  for (auto& x : v) x.depth = mt.depth;
+  std::vector<int> wt(std::max<int64_t>(mt.n_slots / 32, 1), 0);
+  for (int g = 0; g < ntrees; g++)
+    for (int64_t w = so[g] / 32; w < so[g + 1] / 32; w++) wt[w] = g;
+  mt.views.alloc(ntrees, st);
+  mt.slot_off.alloc(ntrees + 1, st);
+  mt.row_off.alloc(ntrees + 1, st);
+  mt.warp_tree.alloc(wt.size(), st);
+  PPTKG_CUDA(cudaMemcpyAsync(mt.views.get(), v.data(), sizeof(TreeView<T, D>) * ntrees, cudaMemcpyHostToDevice, st));
+  PPTKG_CUDA(cudaMemcpyAsync(mt.slot_off.get(), so.data(), sizeof(int64_t) * (ntrees + 1), cudaMemcpyHostToDevice, st));
+  PPTKG_CUDA(cudaMemcpyAsync(mt.row_off.get(), rows, sizeof(int64_t) * (ntrees + 1), cudaMemcpyHostToDevice, st));
+  PPTKG_CUDA(cudaMemcpyAsync(mt.warp_tree.get(), wt.data(), sizeof(int) * wt.size(), cudaMemcpyHostToDevice, st));
+  // the host vectors go out of scope: finish the copies first
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+}
+
+// A stand-in tree carrying the batch-wide traversal bounds for the launch
+// helpers (which size shared memory from the tree they are given).
+static TreeBase* bounds_tree(int depth, int n_nodes) {
+  TreeBase* b = new TreeBase();
+  b->tdepth = depth;
+  b->n_tnodes = n_nodes;
+  return b;
+}
+
+__global__ void k_order_rows(const int* local, int m, int base, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = base + (local ? local[i] : i);
+}
+
+// Rejects index queries outside their own tree's [0, n): one status word for
+// the whole batch, one synchronisation.
+static void check_indices_multi(const TreeBase* const* trees, int ntrees, const int32_t* d_idx, const int64_t* rows,
+                                cudaStream_t st) {
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  for (int g = 0; g < ntrees; g++) {
+    const int64_t m = rows[g + 1] - rows[g];
+    if (m <= 0) continue;
+    k_check_idx<<<div_up(m, 256), 256, 0, st>>>(d_idx + rows[g], (int)m, (int)trees[g]->n, status.get());
+    PPTKG_CHECK_LAUNCH();
+  }
+  int h = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&h, status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h) throw Error(E_RANGE, "query index outside of its tree's [0, n)");
+}
+
+// Processing order of a multi-tree batch: each tree's queries sorted by
+// tree position (as for a single tree) within that tree's rows, so a warp's
+// queries are neighbours.  `spec(g)` gives the QuerySpec of group g.
+template <typename T, int D, typename Spec>
+void multi_order(const TreeBase* const* trees, int ntrees, const int64_t* rows, MultiTables<T, D>& mt, Spec spec,
+                 cudaStream_t st) {
+  const int64_t m_all = rows[ntrees];
+  bool any = false;
+  for (int g = 0; g < ntrees && !any; g++) any = rows[g + 1] - rows[g] >= 2048;
+  if (!any) return;
+  mt.order.alloc(m_all, st);
+  for (int g = 0; g < ntrees; g++) {
+    const int64_t m = rows[g + 1] - rows[g];
+    if (m <= 0) continue;
+    DevBuf<int> local;
+    const int mode = make_order<T, D>(trees[g], spec(g), local, st, true);
+    k_order_rows<<<div_up(m, 256), 256, 0, st>>>(mode == 1 ? local.get() : nullptr, (int)m, (int)rows[g],
+                                                 mt.order.get() + rows[g]);
+    PPTKG_CHECK_LAUNCH();
+  }
+  mt.ordered = true;
+}
+
+template <typename T, int D>
+void multi_knn(const TreeBase* const* trees, int ntrees, const void* d_q, int qdtype, const int64_t* rows, int k,
+               double dmax, int32_t* d_idx, int32_t* d_cnt, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k < 1) throw Error(E_INVALID, "k must be positive");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU kNN kernels");
+  MultiTables<T, D> mt;
+  multi_tables<T, D>(trees, ntrees, rows, mt, st);
+  if (mt.n_slots == 0) return;
+  const size_t qbytes = (qdtype == F64 ? sizeof(double) : sizeof(float)) * D;
+  multi_order<T, D>(trees, ntrees, rows, mt, [&](int g) {
+    QuerySpec qs;
+    qs.pts = (const char*)d_q + rows[g] * qbytes;
+    qs.qdtype = qdtype;
+    qs.m = rows[g + 1] - rows[g];
+    return qs;
+  }, st);
+  std::unique_ptr<TreeBase> bt(bounds_tree(mt.depth, mt.n_nodes));
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  const DistT r2 = radius2<DistT>(dmax);
+  Stage stage("multi.knn", st);
+  if (qdtype == F64)
+    dispatch_knn<T, D>(bt.get(), PointQueries<double, D>{(const double*)d_q}, nullptr, 0, (int)mt.n_slots, k, r2,
+                       d_idx, d_cnt, status.get(), st, mt.map());
+  else
+    dispatch_knn<T, D>(bt.get(), PointQueries<float, D>{(const float*)d_q}, nullptr, 0, (int)mt.n_slots, k, r2, d_idx,
+                       d_cnt, status.get(), st, mt.map());
+  check_status(status.get(), st, "multi-tree knn");
+}
+
+template <typename T>
+void multi_normals(const TreeBase* const* trees, int ntrees, const int32_t* d_idx, const int64_t* rows, int k, float r,
+                   int num_eigen, int precision, double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes,
+                   cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (k < 1) throw Error(E_INVALID, "batched normals need k >= 1");
+  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU normal kernels");
+  MultiTables<T, 3> mt;
+  multi_tables<T, 3>(trees, ntrees, rows, mt, st);
+  if (mt.n_slots == 0) return;
+  // every query index must lie within its own tree's input rows
+  check_indices_multi(trees, ntrees, d_idx, rows, st);
+  multi_order<T, 3>(trees, ntrees, rows, mt, [&](int g) {
+    QuerySpec qs;
+    qs.idx = d_idx + rows[g];
+    qs.m = rows[g + 1] - rows[g];
+    qs.exclude_self = false;
+    return qs;
+  }, st);
+  std::unique_ptr<TreeBase> bt(bounds_tree(mt.depth, mt.n_nodes));
+  DevBuf<int> status(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  const DistT rr = (DistT)(T)r;
+  const DistT r2 = rr * rr;
+  int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
+  Stage stage("multi.normals", st);
+  // fwd comes from each warp's TreeView (null here)
+  dispatch_normals<T, IndexQueries<3, false>>(bt.get(), IndexQueries<3, false>{d_idx, nullptr}, nullptr, 0,
+                                              (int)mt.n_slots, k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals,
+                                              d_sizes, status.get(), st, mt.map());
+  check_status(status.get(), st, "multi-tree normals");
+}
+
+template void multi_knn<float, 3>(const TreeBase* const*, int, const void*, int, const int64_t*, int, double, int32_t*,
+                                  int32_t*, cudaStream_t);
+template void multi_knn<double, 3>(const TreeBase* const*, int, const void*, int, const int64_t*, int, double,
+                                   int32_t*, int32_t*, cudaStream_t);
+template void multi_normals<float>(const TreeBase* const*, int, const int32_t*, const int64_t*, int, float, int, int,
+                                   double, float*, float*, int32_t*, cudaStream_t);
+template void multi_normals<double>(const TreeBase* const*, int, const int32_t*, const int64_t*, int, float, int, int,
+                                    double, double*, double*, int32_t*, cudaStream_t);
+
 // ------------------------------------------- allocation-free normals ----
 // Scratch of pptkg_tree_normals_noalloc, resident on every GPU that loads the
 // library: [0] status word, [1] FP64 re-solve queue length, then (from int 64,
@@ -967,8 +1171,8 @@ static void normals_noalloc_k(const TreeBase* t, const int32_t* idx, int m, int 
   }
   launch_normals<T, KMAX, L, PREC_FP32>(t, ld, nullptr, mode, m, k, r2, num_eigen, 1e-3, ev, ew, sz, fix, nfix,
                                         status, st);
-  k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, t->fwd, fix, nfix, num_eigen,
-                                                      ev, ew, sz);
+  k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, fix, nfix, num_eigen, ev, ew,
+                                                      sz, nullptr);
   PPTKG_CHECK_LAUNCH();
 }
 

@@ -50,6 +50,16 @@ template <typename T>
 void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
                     T* d_evals, int32_t* d_sizes, cudaStream_t st);
 
+// One launch over several single trees: tree g answers the query rows
+// [rows[g], rows[g+1]) (host offsets) of a concatenated batch.
+template <typename T, int D>
+void multi_knn(const TreeBase* const* trees, int ntrees, const void* d_q, int qdtype, const int64_t* rows, int k,
+               double dmax, int32_t* d_idx, int32_t* d_cnt, cudaStream_t st);
+template <typename T>
+void multi_normals(const TreeBase* const* trees, int ntrees, const int32_t* d_idx, const int64_t* rows, int k, float r,
+                   int num_eigen, int precision, double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes,
+                   cudaStream_t st);
+
 // pptkg_tree_normals_noalloc: the tree-normals path with its scratch in a
 // static device array instead of allocated memory (device pointers only).
 template <typename T>

@@ -1,0 +1,323 @@
+"""Continuous-batching server for resident k-d trees.
+
+Trees built through the server stay in HBM.  Build, kNN, r-near and normal
+requests of very different sizes are admitted first-in first-out against an
+HBM budget; whenever an execution slot frees up, every admitted query request
+is folded into the next batch -- kNN requests (same k, dmax, query dtype)
+across all trees become one multi-tree launch, normal requests likewise --
+and the batch runs on that slot's CUDA stream while other slots keep
+running.  A request's answer does not depend on what it was batched with:
+the multi-tree kernels give every query exactly the result it gets alone.
+
+The engine that executes batches is pluggable (``GpuEngine`` by default), so
+the scheduling logic can be exercised without a GPU.
+"""
+import math
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+
+import numpy as np
+
+# Bytes per point of a resident tree (tree-ordered points with index 16 B,
+# forward map 4 B, build records and traversal nodes ~48 B) and of a build's
+# transient scratch; bytes per query of a batch.
+TREE_BYTES_PER_POINT = 72
+BUILD_SCRATCH_PER_POINT = 160
+QUERY_BYTES = 96
+
+
+class Request:
+    __slots__ = ("kind", "args", "future", "t_submit", "t_start", "t_done", "bytes", "m", "key")
+
+    def __init__(self, kind, args, nbytes, m, key=None):
+        self.kind = kind
+        self.args = args
+        self.future = Future()
+        self.t_submit = time.perf_counter()
+        self.t_start = None
+        self.t_done = None
+        self.bytes = nbytes
+        self.m = m
+        self.key = key
+
+
+class GpuEngine:
+    """Executes batches with the native library on one device."""
+
+    def __init__(self, device=0):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+
+    def stream(self):
+        return self.torch.cuda.Stream(device=self.device)
+
+    def build(self, points, maxleafsize, emptysplit, stream):
+        from . import kdtree
+        with self.torch.cuda.stream(stream):
+            return kdtree._build(points, maxleafsize=maxleafsize, emptysplit=emptysplit)
+
+    @staticmethod
+    def _merge(trees, parts):
+        """Requests on the same tree become one group of the launch: returns
+        the distinct trees, each one's concatenated parts, and for every
+        request its (group, first row, rows)."""
+        order, where = {}, []
+        for t, x in zip(trees, parts):
+            g = order.setdefault(id(t), len(order))
+            where.append(g)
+        uniq = [None] * len(order)
+        groups = [[] for _ in order]
+        for t, x, g in zip(trees, parts, where):
+            uniq[g] = t
+            groups[g].append(x)
+        lens = [[len(x) for x in grp] for grp in groups]
+        starts = np.concatenate([[0], np.cumsum([sum(l) for l in lens])]).astype(np.int64)
+        cursor = [int(starts[g]) for g in range(len(uniq))]
+        spans = []
+        for x, g in zip(parts, where):
+            spans.append((cursor[g], len(x)))
+            cursor[g] += len(x)
+        return uniq, groups, starts, spans
+
+    def knn_batch(self, trees, queries, k, dmax, stream):
+        """queries: list of per-request query arrays (numpy or CUDA tensors);
+        requests on the same tree share one group of the launch."""
+        import ctypes
+        from . import _native as N
+        torch = self.torch
+        with torch.cuda.stream(stream):
+            qs = [torch.as_tensor(q, device=self.device) for q in queries]
+            dt = qs[0].dtype if qs[0].dtype in (torch.float32, torch.float64) else torch.float64
+            uniq, groups, rows, spans = self._merge(trees, qs)
+            q = torch.cat([x.to(dt) for grp in groups for x in grp]).contiguous()
+            m = int(rows[-1])
+            idx = torch.empty((m, k), dtype=torch.int32, device=self.device)
+            cnt = torch.empty((m,), dtype=torch.int32, device=self.device)
+            handles = (ctypes.c_void_p * len(uniq))(*[t._h.value for t in uniq])
+            N.call("pptkg_multi_knn", handles, len(uniq), N.ptr(q), N.ptr(rows), 0 if dt == torch.float32 else 1,
+                   N.MEM_DEVICE, int(k), float(np.float32(dmax)), N.ptr(idx), N.ptr(cnt),
+                   ctypes.c_void_p(stream.cuda_stream), where="serving knn")
+        return [(idx[a:a + n], cnt[a:a + n]) for a, n in spans]
+
+    def normals_batch(self, trees, indices, k, r, precision, stream):
+        import ctypes
+        from . import _native as N
+        from .estimate_normals import PRECISIONS
+        torch = self.torch
+        with torch.cuda.stream(stream):
+            ids = []
+            for t, ix in zip(trees, indices):
+                if ix is None:
+                    ix = torch.arange(t.n, dtype=torch.int32, device=self.device)
+                ids.append(torch.as_tensor(ix, device=self.device).to(torch.int32))
+            uniq, groups, rows, spans = self._merge(trees, ids)
+            q = torch.cat([x for grp in groups for x in grp]).contiguous()
+            m = int(rows[-1])
+            tdt = torch.float32 if trees[0].dtype == np.float32 else torch.float64
+            ev = torch.empty((m, 3), dtype=tdt, device=self.device)
+            handles = (ctypes.c_void_p * len(uniq))(*[t._h.value for t in uniq])
+            N.call("pptkg_multi_normals", handles, len(uniq), N.ptr(q), N.ptr(rows), N.MEM_DEVICE, int(k),
+                   ctypes.c_float(float(np.float32(r))), 1, PRECISIONS[precision], N.ptr(ev), None, None,
+                   ctypes.c_void_p(stream.cuda_stream), where="serving normals")
+        return [ev[a:a + n] for a, n in spans]
+
+    def rnear(self, tree, queries, dmax, stream):
+        from . import kdtree
+        with self.torch.cuda.stream(stream):
+            q = self.torch.as_tensor(queries, device=self.device)
+            return kdtree.rnear(tree, q, dmax)
+
+    def synchronize(self, stream):
+        stream.synchronize()
+
+
+class Server:
+    """Continuous-batching server.
+
+    budget_bytes: HBM the server may commit to resident trees plus the
+        transient needs of admitted requests.
+    slots: batches that may run at once, each on its own CUDA stream.
+    max_batch_queries: upper bound on the queries folded into one batch.
+    """
+
+    def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=8_000_000, engine=None):
+        self.budget = float(budget_bytes)
+        self.engine = engine or GpuEngine(device)
+        self.max_batch = int(max_batch_queries)
+        self.trees = {}
+        self.tree_bytes = {}
+        self._next_id = 0
+        self._pending = deque()
+        self._committed = 0.0
+        self._cv = threading.Condition()
+        self._free = [self.engine.stream() for _ in range(slots)]
+        self._running = True
+        self._done = []
+        self._batches = 0
+        self._thread = threading.Thread(target=self._loop, name="pptk-b200-server", daemon=True)
+        self._thread.start()
+
+    # ------------------------------------------------------------ requests --
+    def build(self, points, maxleafsize=10, emptysplit=0.2):
+        """Future of a tree id."""
+        n = int(points.shape[0])
+        r = Request("build", (points, maxleafsize, emptysplit), n * (TREE_BYTES_PER_POINT + BUILD_SCRATCH_PER_POINT), n)
+        return self._submit(r)
+
+    def knn(self, tree_id, queries, k=1, dmax=math.inf):
+        """Future of (indices m x k, counts m) for point queries."""
+        m = int(queries.shape[0])
+        dt = str(getattr(queries, "dtype", "float64"))
+        r = Request("knn", (tree_id, queries), m * (QUERY_BYTES + 4 * int(k)), m, key=("knn", int(k), float(dmax), dt))
+        return self._submit(r)
+
+    def normals(self, tree_id, indices=None, k=16, r=math.inf, precision="auto"):
+        """Future of the normals (m x 3) of the tree's input rows `indices`
+        (all rows when None), over k nearest neighbours within r."""
+        m = self.trees[tree_id].n if indices is None else int(len(indices))
+        req = Request("normals", (tree_id, indices), m * (QUERY_BYTES + 4 * int(k)), m,
+                      key=("normals", int(k), float(r), precision))
+        return self._submit(req)
+
+    def rnear(self, tree_id, queries, dmax):
+        m = int(queries.shape[0])
+        return self._submit(Request("rnear", (tree_id, queries, float(dmax)), m * QUERY_BYTES * 8, m))
+
+    def drop(self, tree_id):
+        """Releases a resident tree."""
+        with self._cv:
+            self.trees.pop(tree_id, None)
+            self._committed -= self.tree_bytes.pop(tree_id, 0)
+            self._cv.notify_all()
+
+    def _submit(self, r):
+        if r.bytes > self.budget:
+            r.future.set_exception(MemoryError(f"request needs {r.bytes:.3g} B, above the budget {self.budget:.3g} B"))
+            return r.future
+        with self._cv:
+            if not self._running:
+                raise RuntimeError("server closed")
+            self._pending.append(r)
+            self._cv.notify_all()
+        return r.future
+
+    # ----------------------------------------------------------- scheduler --
+    def _admit(self):
+        """FIFO admission under the budget.  A build or r-near request runs
+        as a batch of its own; consecutive kNN / normal requests are folded
+        into one batch up to max_batch_queries."""
+        out = []
+        queries = 0
+        while self._pending:
+            r = self._pending[0]
+            if r.kind != "build" and r.args[0] not in self.trees:
+                self._pending.popleft()
+                r.future.set_exception(KeyError(f"unknown tree {r.args[0]}"))
+                continue
+            exclusive = r.kind in ("build", "rnear")
+            if out and (exclusive or queries + r.m > self.max_batch):
+                break
+            if self._committed + r.bytes > self.budget:
+                break
+            self._pending.popleft()
+            self._committed += r.bytes
+            out.append(r)
+            queries += r.m
+            if exclusive:
+                break
+        return out
+
+    def _loop(self):
+        while True:
+            with self._cv:
+                while self._running and (not self._pending or not self._free):
+                    self._cv.wait(0.01)
+                if not self._running and not self._pending:
+                    return
+                if not self._free:
+                    continue
+                batch = self._admit()
+                if not batch:
+                    self._cv.wait(0.001)
+                    continue
+                stream = self._free.pop()
+                self._batches += 1
+            threading.Thread(target=self._run, args=(batch, stream), daemon=True).start()
+
+    def _run(self, batch, stream):
+        t0 = time.perf_counter()
+        for r in batch:
+            r.t_start = t0
+        try:
+            groups = {}
+            for r in batch:
+                groups.setdefault(r.key if r.key else (r.kind, id(r)), []).append(r)
+            for key, rs in groups.items():
+                kind = rs[0].kind
+                if kind == "build":
+                    r = rs[0]
+                    tree = self.engine.build(*r.args, stream)
+                    with self._cv:
+                        tid = self._next_id
+                        self._next_id += 1
+                        self.trees[tid] = tree
+                        self.tree_bytes[tid] = r.m * TREE_BYTES_PER_POINT
+                        self._committed += self.tree_bytes[tid]
+                    self._finish([r], [tid], stream)
+                elif kind == "knn":
+                    trees = [self.trees[r.args[0]] for r in rs]
+                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], key[1], key[2], stream)
+                    self._finish(rs, res, stream)
+                elif kind == "normals":
+                    trees = [self.trees[r.args[0]] for r in rs]
+                    res = self.engine.normals_batch(trees, [r.args[1] for r in rs], key[1], key[2], key[3], stream)
+                    self._finish(rs, res, stream)
+                elif kind == "rnear":
+                    r = rs[0]
+                    res = self.engine.rnear(self.trees[r.args[0]], r.args[1], r.args[2], stream)
+                    self._finish([r], [res], stream)
+        except Exception as e:  # a failed batch fails its requests, not the server
+            for r in batch:
+                if not r.future.done():
+                    r.future.set_exception(e)
+        finally:
+            with self._cv:
+                for r in batch:
+                    self._committed -= r.bytes
+                self._free.append(stream)
+                self._cv.notify_all()
+
+    def _finish(self, rs, results, stream):
+        self.engine.synchronize(stream)
+        t = time.perf_counter()
+        for r, res in zip(rs, results):
+            r.t_done = t
+            with self._cv:
+                self._done.append((r.kind, r.m, r.t_submit, r.t_done))
+            r.future.set_result(res)
+
+    # --------------------------------------------------------------- info --
+    def stats(self, since=0.0):
+        """Per-kind request count, queries, p50/p99 latency (s) and queries/s
+        over the requests finished after `since` (perf_counter time)."""
+        with self._cv:
+            done = [d for d in self._done if d[3] >= since]
+        out = {}
+        for kind in sorted({d[0] for d in done}):
+            ds = [d for d in done if d[0] == kind]
+            lat = np.array([d[3] - d[2] for d in ds])
+            q = sum(d[1] for d in ds)
+            span = max(d[3] for d in ds) - min(d[2] for d in ds)
+            out[kind] = {"requests": len(ds), "queries": q, "p50_s": float(np.percentile(lat, 50)),
+                         "p99_s": float(np.percentile(lat, 99)), "queries_per_s": q / span if span > 0 else None}
+        out["batches"] = self._batches
+        return out
+
+    def close(self):
+        with self._cv:
+            self._running = False
+            self._cv.notify_all()
+        self._thread.join(timeout=30)
