@@ -82,9 +82,20 @@ class GpuEngine:
             cursor[g] += len(x)
         return uniq, groups, starts, spans
 
-    def knn_batch(self, trees, queries, k, dmax, stream):
+    def _to_host(self, tensors):
+        """Pinned host copies on the current stream (complete once the
+        stream is synchronised), as numpy arrays."""
+        out = []
+        for t in tensors:
+            h = self.torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t, non_blocking=True)
+            out.append(h.numpy())
+        return out
+
+    def knn_batch(self, trees, queries, k, dmax, stream, host=False):
         """queries: list of per-request query arrays (numpy or CUDA tensors);
-        requests on the same tree share one group of the launch."""
+        requests on the same tree share one group of the launch.  host: the
+        results come back as numpy arrays (copied on this stream)."""
         import ctypes
         from . import _native as N
         torch = self.torch
@@ -100,9 +111,11 @@ class GpuEngine:
             N.call("pptkg_multi_knn", handles, len(uniq), N.ptr(q), N.ptr(rows), 0 if dt == torch.float32 else 1,
                    N.MEM_DEVICE, int(k), float(np.float32(dmax)), N.ptr(idx), N.ptr(cnt),
                    ctypes.c_void_p(stream.cuda_stream), where="serving knn")
+            if host:
+                idx, cnt = self._to_host([idx, cnt])
         return [(idx[a:a + n], cnt[a:a + n]) for a, n in spans]
 
-    def normals_batch(self, trees, indices, k, r, precision, stream):
+    def normals_batch(self, trees, indices, k, r, precision, stream, host=False):
         import ctypes
         from . import _native as N
         from .estimate_normals import PRECISIONS
@@ -122,6 +135,8 @@ class GpuEngine:
             N.call("pptkg_multi_normals", handles, len(uniq), N.ptr(q), N.ptr(rows), N.MEM_DEVICE, int(k),
                    ctypes.c_float(float(np.float32(r))), 1, PRECISIONS[precision], N.ptr(ev), None, None,
                    ctypes.c_void_p(stream.cuda_stream), where="serving normals")
+            if host:
+                ev, = self._to_host([ev])
         return [ev[a:a + n] for a, n in spans]
 
     def rnear(self, tree, queries, dmax, stream):
@@ -167,19 +182,25 @@ class Server:
         r = Request("build", (points, maxleafsize, emptysplit), n * (TREE_BYTES_PER_POINT + BUILD_SCRATCH_PER_POINT), n)
         return self._submit(r)
 
-    def knn(self, tree_id, queries, k=1, dmax=math.inf):
-        """Future of (indices m x k, counts m) for point queries."""
+    def knn(self, tree_id, queries, k=1, dmax=math.inf, to_host=None):
+        """Future of (indices m x k, counts m) for point queries.  to_host:
+        numpy results (default: when the queries are a numpy array),
+        otherwise CUDA tensors."""
         m = int(queries.shape[0])
         dt = str(getattr(queries, "dtype", "float64"))
-        r = Request("knn", (tree_id, queries), m * (QUERY_BYTES + 4 * int(k)), m, key=("knn", int(k), float(dmax), dt))
+        host = isinstance(queries, np.ndarray) if to_host is None else bool(to_host)
+        r = Request("knn", (tree_id, queries), m * (QUERY_BYTES + 4 * int(k)), m,
+                    key=("knn", int(k), float(dmax), dt, host))
         return self._submit(r)
 
-    def normals(self, tree_id, indices=None, k=16, r=math.inf, precision="auto"):
+    def normals(self, tree_id, indices=None, k=16, r=math.inf, precision="auto", to_host=None):
         """Future of the normals (m x 3) of the tree's input rows `indices`
-        (all rows when None), over k nearest neighbours within r."""
+        (all rows when None), over k nearest neighbours within r.  to_host
+        as for knn (default: when the indices are a numpy array)."""
         m = self.trees[tree_id].n if indices is None else int(len(indices))
+        host = isinstance(indices, np.ndarray) if to_host is None else bool(to_host)
         req = Request("normals", (tree_id, indices), m * (QUERY_BYTES + 4 * int(k)), m,
-                      key=("normals", int(k), float(r), precision))
+                      key=("normals", int(k), float(r), precision, host))
         return self._submit(req)
 
     def rnear(self, tree_id, queries, dmax):
@@ -269,11 +290,13 @@ class Server:
                     self._finish([r], [tid], stream)
                 elif kind == "knn":
                     trees = [self.trees[r.args[0]] for r in rs]
-                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], key[1], key[2], stream)
+                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], key[1], key[2], stream,
+                                                host=key[4])
                     self._finish(rs, res, stream)
                 elif kind == "normals":
                     trees = [self.trees[r.args[0]] for r in rs]
-                    res = self.engine.normals_batch(trees, [r.args[1] for r in rs], key[1], key[2], key[3], stream)
+                    res = self.engine.normals_batch(trees, [r.args[1] for r in rs], key[1], key[2], key[3], stream,
+                                                    host=key[4])
                     self._finish(rs, res, stream)
                 elif kind == "rnear":
                     r = rs[0]

@@ -149,3 +149,23 @@ def ragged_clouds(count=4096, lo=1000, hi=200000, seed=4):
         plane = uv[:, :1] * a + uv[:, 1:] * b + rng.normal(0, 0.01, (n_plane, 1)) * nrm
         out[off[i]:off[i + 1]] = np.concatenate([blobs, plane])
     return out, off
+
+
+def request_mix(n_points, per_kind, seed=10, lo=1000, hi=1_000_000):
+    """Seeded request stream over an n-point scene: alternating kNN and
+    normal requests with query counts log-uniform in [lo, hi], until each
+    kind totals `per_kind` queries.  Returns [(kind, rows)] with rows the
+    int32 scene rows a request asks about (kNN requests query those points'
+    coordinates, normal requests those rows)."""
+    rng = np.random.default_rng(seed)
+    left = {"knn": int(per_kind), "normals": int(per_kind)}
+    out = []
+    kind = "knn"
+    while left["knn"] > 0 or left["normals"] > 0:
+        if left[kind] > 0:
+            m = int(np.exp(rng.uniform(math.log(lo), math.log(hi))))
+            m = max(1, min(m, left[kind]))
+            out.append((kind, rng.integers(0, n_points, m).astype(np.int32)))
+            left[kind] -= m
+        kind = "normals" if kind == "knn" else "knn"
+    return out

@@ -54,6 +54,10 @@ def test_multi_tree_normals_equal_single_tree(gpu):
         assert np.array_equal(ev[rows[g]:rows[g + 1]], alone)
 
 
+def _np(x):
+    return x.cpu().numpy() if hasattr(x, "cpu") else np.asarray(x)
+
+
 def test_server_answers_are_the_same_alone_and_in_the_mix(gpu):
     import torch
     from pptk_b200 import serving
@@ -70,6 +74,8 @@ def test_server_answers_are_the_same_alone_and_in_the_mix(gpu):
         else:
             ix = rng.integers(0, len(clouds[g]), int(rng.integers(1, 20_000))).astype(np.int32)
             reqs.append(("normals", g, ix))
+    # every third request passes CUDA tensors (and gets CUDA tensors back)
+    reqs = [(kind, g, torch.from_numpy(a).cuda() if j % 3 == 0 else a) for j, (kind, g, a) in enumerate(reqs)]
     results = [None] * len(reqs)
 
     def client(lo, hi):
@@ -84,13 +90,16 @@ def test_server_answers_are_the_same_alone_and_in_the_mix(gpu):
     st = srv.stats()
     assert st["knn"]["requests"] == 20 and st["normals"]["requests"] == 20
     # alone: the same requests one at a time
-    for (kind, g, a), got in zip(reqs, results):
+    for j, ((kind, g, a), got) in enumerate(zip(reqs, results)):
         f = srv.knn(ids[g], a, k=8) if kind == "knn" else srv.normals(ids[g], a, k=8)
         alone = f.result(timeout=120)
+        on_device = j % 3 == 0
         if kind == "knn":
-            assert torch.equal(got[0], alone[0]) and torch.equal(got[1], alone[1])
-            direct, _ = gpu.kdtree.knn(srv.trees[ids[g]], a, 8)
-            assert np.array_equal(got[0].cpu().numpy(), direct)
+            assert all(torch.is_tensor(x) == on_device for x in got)
+            assert np.array_equal(_np(got[0]), _np(alone[0])) and np.array_equal(_np(got[1]), _np(alone[1]))
+            direct, _ = gpu.kdtree.knn(srv.trees[ids[g]], _np(a), 8)
+            assert np.array_equal(_np(got[0]), direct)
         else:
-            assert torch.equal(got, alone)
+            assert torch.is_tensor(got) == on_device
+            assert np.array_equal(_np(got), _np(alone))
     srv.close()

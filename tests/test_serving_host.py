@@ -31,7 +31,7 @@ class FakeEngine:
         time.sleep(self.delay)
         return FakeTree(points)
 
-    def knn_batch(self, trees, queries, k, dmax, stream):
+    def knn_batch(self, trees, queries, k, dmax, stream, host=False):
         with self.lock:
             self.batches.append(("knn", len(trees)))
         time.sleep(self.delay)
@@ -42,7 +42,7 @@ class FakeEngine:
             out.append((idx, np.full(len(q), min(k, t.n), np.int32)))
         return out
 
-    def normals_batch(self, trees, indices, k, r, precision, stream):
+    def normals_batch(self, trees, indices, k, r, precision, stream, host=False):
         with self.lock:
             self.batches.append(("normals", len(trees)))
         return [np.zeros((t.n if i is None else len(i), 3)) for t, i in zip(trees, indices)]
