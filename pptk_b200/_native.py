@@ -64,6 +64,8 @@ SIGNATURES = {
     "pptkg_multi_normals": [_vp, _int, _vp, _vp, _int, _int, _flt, _int, _int, _vp, _vp, _vp, _vp],
     "pptkg_profile_enable": [_int],
     "pptkg_profile_get": [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), _pi64],
+    "pptkg_tune_set": [ctypes.c_char_p, _i64],
+    "pptkg_tune_get": [ctypes.c_char_p, _pi64],
 }
 
 _lib = None
@@ -145,3 +147,14 @@ def ptr(a):
     if isinstance(a, np.ndarray):
         return ctypes.c_void_p(a.ctypes.data)
     return ctypes.c_void_p(a.data_ptr())
+
+
+def tune_set(name, value):
+    """Sets a process-wide tuning knob of the native library (pptkg_tune_set)."""
+    call("pptkg_tune_set", name.encode(), int(value))
+
+
+def tune_get(name):
+    v = ctypes.c_int64()
+    call("pptkg_tune_get", name.encode(), ctypes.byref(v))
+    return v.value

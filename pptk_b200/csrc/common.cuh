@@ -40,6 +40,11 @@ enum Status {
 
 // Counts every kernel launch of the library (pptkg_launch_count) and checks it.
 extern std::atomic<long long> g_launches;
+
+// Run-time tuning knobs (pptkg_tune_set / pptkg_tune_get), read at launch.
+//  lane_span: a kNN warp whose queries span more than this many tree
+//    positions walks the tree per lane instead of as a packet (-1: never).
+extern std::atomic<int> g_tune_lane_span;
 #define PPTKG_CHECK_LAUNCH()          \
   do {                                \
     ::pptkg::g_launches++;            \

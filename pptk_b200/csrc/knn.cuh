@@ -89,8 +89,19 @@ struct TopK<KMAX, float> {
     }
     s[KMAX - 1] = s[KMAX - 1] > c ? c : s[KMAX - 1];
   }
+  // Lowers the bound of the k live slots to b, inclusively (distances equal
+  // to b still enter): the seed key sorts after every real key of distance b.
+  // Only valid when at least k real candidates with distance <= b exist, so
+  // that every seed key is pushed out by the end of the search.
+  __device__ __forceinline__ void seed(int k, float b, float) {
+    const unsigned long long key = ((unsigned long long)__float_as_uint(b) << 32) | 0xffffffffull;
+    if (!(b >= 0.f) || key >= lim) return;
+#pragma unroll
+    for (int j = 0; j < KMAX; j++)
+      if (j < k) s[j] = key;
+  }
   __device__ __forceinline__ void reserve(int) {}
-  __device__ __forceinline__ bool valid(int j) const { return s[j] < lim; }
+  __device__ __forceinline__ bool valid(int j) const { return s[j] < lim && (unsigned)s[j] != 0xffffffffu; }
   __device__ __forceinline__ int pos(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
   __device__ __forceinline__ float dist(int j) const { return __uint_as_float((unsigned)(s[j] >> 32)); }
 };
@@ -127,8 +138,18 @@ struct TopK<KMAX, double> {
       p[KMAX - 1] = cp;
     }
   }
+  // As TopK<KMAX, float>::seed; r2 is the bound the slots were reset to.
+  __device__ __forceinline__ void seed(int k, double b, double r2) {
+    if (!(b >= 0.0) || !(b < r2)) return;
+#pragma unroll
+    for (int j = 0; j < KMAX; j++)
+      if (j < k) {
+        d[j] = b;
+        p[j] = 0x7fffffff;
+      }
+  }
   __device__ __forceinline__ void reserve(int) {}
-  __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && d[j] >= 0.0; }
+  __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && p[j] != 0x7fffffff && d[j] >= 0.0; }
   __device__ __forceinline__ int pos(int j) const { return p[j]; }
   __device__ __forceinline__ double dist(int j) const { return d[j]; }
 };
@@ -315,6 +336,87 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
     if (!found) break;
   }
   return ok;
+}
+
+// Per-lane traversal for warps whose queries lie far apart, where a packet
+// walk would visit the union of 32 unrelated paths one node at a time.  Each
+// lane walks its own near-first depth-first path with a private stack of
+// deferred children (reference, size and box distance, re-tested on pop), so
+// the 32 walks advance side by side and their node loads overlap.  The set of
+// candidates each query accepts is the same as in the packet walk: every
+// point whose distance is within the query's final bound is offered, so the
+// result (the k smallest (dist2, position) pairs) is identical.
+// Requires tv.depth <= LSTACK (the caller checks); false on a corrupt tree.
+template <int LSTACK, typename T, int D, typename DistT, typename Top>
+__device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top) {
+  if (!active) return true;
+  int sref[LSTACK], scnt[LSTACK];
+  DistT smd[LSTACK];
+  int sp = 0;
+  auto need = [&](DistT md) { return md < r2 && md <= top.worst(); };
+  auto scan = [&](int begin, int count) {
+    for (int p = begin; p < begin + count; p++) {
+      const PointRec<T, D> pr = tv.pts[p];
+      const DistT d2 = point_dist2<T, DistT, D>(pr.c, q);
+      if (d2 <= top.worst() && d2 < r2 && p != own) top.offer(d2, p);
+    }
+  };
+  int cur = tv.root, visits = 0;
+  while (true) {
+    if (++visits > tv.n_nodes) return false;  // a tree is acyclic: more visits mean a corrupt node array
+    const TNode<T, D> nd = load_node(tv.nodes, cur);
+    const DistT md0 = nd.cnt[0] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], q) : (DistT)INFINITY;
+    const DistT md1 = nd.cnt[1] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) : (DistT)INFINITY;
+    const bool sw = md1 < md0;
+    const DistT mdn = sw ? md1 : md0, mdf = sw ? md0 : md1;
+    const int refn = sw ? nd.ref[1] : nd.ref[0], reff = sw ? nd.ref[0] : nd.ref[1];
+    const int cntn = sw ? nd.cnt[1] : nd.cnt[0], cntf = sw ? nd.cnt[0] : nd.cnt[1];
+    int next = -1;
+    // the far child is never nearer than the near one, so it is needed only
+    // when the near one is
+    if (need(mdn)) {
+      if (refn >= 0) {
+        next = refn;
+        if (need(mdf)) {
+          if (sp >= LSTACK) return false;
+          sref[sp] = reff;
+          scnt[sp] = cntf;
+          smd[sp] = mdf;
+          sp++;
+        }
+      } else {
+        scan(-refn - 1, cntn);
+        if (need(mdf)) {
+          if (reff >= 0)
+            next = reff;
+          else
+            scan(-reff - 1, cntf);
+        }
+      }
+    }
+    while (next < 0 && sp > 0) {
+      --sp;
+      if (!need(smd[sp])) continue;
+      if (sref[sp] < 0)
+        scan(-sref[sp] - 1, scnt[sp]);
+      else
+        next = sref[sp];
+    }
+    if (next < 0) return true;
+    cur = next;
+  }
+}
+
+// Warp-uniform choice of the traversal: per-lane walks when the warp's
+// queries span more than `span` tree positions (anchors: tree positions near
+// each query; -1 unknown), packet walks otherwise.
+template <int LSTACK>
+__device__ __forceinline__ bool use_lane_walk(int anchor, bool active, int span, int depth) {
+  const unsigned FULL = 0xffffffffu;
+  const bool known = active && anchor >= 0;
+  const int lo = __reduce_min_sync(FULL, known ? anchor : 0x7fffffff);
+  const int hi = __reduce_max_sync(FULL, known ? anchor : -1);
+  return span >= 0 && depth <= LSTACK && hi > lo && hi - lo > span;
 }
 
 // r-near over the whole tree in ascending tree position (the reference's

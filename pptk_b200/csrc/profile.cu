@@ -11,6 +11,7 @@
 namespace pptkg {
 
 std::atomic<long long> g_launches{0};
+std::atomic<int> g_tune_lane_span{512};
 
 namespace {
 struct Pending {
@@ -83,5 +84,24 @@ int pptkg_profile_get(const char* stage, double* total_ms, int64_t* count) {
 }
 
 int64_t pptkg_launch_count(void) { return pptkg::g_launches.load(); }
+
+int pptkg_tune_set(const char* name, int64_t value) {
+  if (!name) return PPTKG_E_INVALID;
+  if (std::string(name) == "lane_span") {
+    if (value < -1 || value > INT32_MAX) return PPTKG_E_INVALID;
+    pptkg::g_tune_lane_span.store((int)value);
+    return PPTKG_OK;
+  }
+  return PPTKG_E_INVALID;
+}
+
+int pptkg_tune_get(const char* name, int64_t* value) {
+  if (!name || !value) return PPTKG_E_INVALID;
+  if (std::string(name) == "lane_span") {
+    *value = pptkg::g_tune_lane_span.load();
+    return PPTKG_OK;
+  }
+  return PPTKG_E_INVALID;
+}
 
 }  // extern "C"

@@ -61,14 +61,19 @@ __host__ __device__ constexpr int normals_logcap(int kmax) { return 2 * kmax; }
 
 // ------------------------------------------------------------- loaders ----
 // Query i is row i of a user array.
+// `anc` (optional): per query row, a tree position near the query (the start
+// of the leaf the query falls in), used to seed the search radius.
 template <typename Q, int D>
 struct PointQueries {
   const Q* q;
+  const int* anc = nullptr;
   template <typename T, typename DistT>
-  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own) const {
+  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own,
+                                       int* anchor = nullptr) const {
 #pragma unroll
     for (int d = 0; d < D; d++) out[d] = (DistT)q[(int64_t)i * D + d];
     own = -1;
+    if (anchor) *anchor = anc ? anc[i] : -1;
     return true;
   }
 };
@@ -81,10 +86,12 @@ struct IndexQueries {
   const int* idx;
   const int* fwd;
   template <typename T, typename DistT>
-  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own) const {
+  __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own,
+                                       int* anchor = nullptr) const {
     const int o = idx ? idx[i] : i;
     const int p = (fwd ? fwd : tv.fwd)[o];
     own = -1;
+    if (anchor) *anchor = p;
     if (p < 0) return false;  // the point was dropped (NaN/inf): no neighbours
     const PointRec<T, D> r = tv.pts[p];
 #pragma unroll
@@ -126,6 +133,55 @@ __device__ __forceinline__ int forest_query(int slot, const SlotMap& fm, TreeVie
   return p < fm.valid_off[c + 1] ? tv.pts[p].id : -1;
 }
 
+// Per-lane stack capacity of the per-lane walk (trees deeper than this use
+// packet walks only).
+constexpr int LANE_STACK = 64;
+
+// Upper bound on the k-th smallest squared distance from q to the points of
+// the tree positions [lo, hi) other than `own`: for a window of w consecutive
+// positions containing `anchor` (w = k, plus one when `own` is excluded and
+// then skipped), the largest distance from q to its points is such a bound;
+// the smallest over three windows is returned.  Infinity when the range
+// holds fewer than w points.  Distances use the same arithmetic as the
+// search, so the bound is attained exactly by a real candidate.
+template <typename T, int D, typename DistT>
+__device__ __forceinline__ DistT seed_bound(const TreeView<T, D>& tv, const DistT* q, int anchor, int k, int own,
+                                            int lo, int hi) {
+  // three windows of w positions: ending at, centred on and starting at the
+  // anchor (clamped to [lo, hi)); each gives a bound, the smallest is kept
+  const int w = k + (own >= 0 ? 1 : 0);
+  if (hi - lo < w || anchor < 0) return (DistT)INFINITY;
+  const int a = min(max(anchor, lo), hi - 1);
+  const int b0 = min(max(a - w + 1, lo), hi - w);
+  const int b1 = min(max(a - w / 2, lo), hi - w);
+  const int b2 = min(max(a, lo), hi - w);
+  DistT m0 = (DistT)0, m1 = (DistT)0, m2 = (DistT)0;
+  for (int p = b0; p < b2 + w; p++) {
+    if (p == own) continue;
+    const DistT d2 = point_dist2<T, DistT, D>(tv.pts[p].c, q);
+    if (p < b0 + w) m0 = d2 > m0 ? d2 : m0;
+    if (p >= b1 && p < b1 + w) m1 = d2 > m1 ? d2 : m1;
+    if (p >= b2) m2 = d2 > m2 ? d2 : m2;
+  }
+  const DistT m01 = m0 < m1 ? m0 : m1;
+  return m01 < m2 ? m01 : m2;
+}
+
+// Seeds a query's top-k bound from its neighbourhood in tree order.  Keeps a
+// warp of far-apart queries from visiting most of the tree before each
+// query's list fills up.
+template <typename T, int D, typename DistT, typename Top>
+__device__ __forceinline__ void seed_topk(Top& top, const TreeView<T, D>& tv, const SlotMap& fm, int slot,
+                                          const DistT* q, int anchor, int k, int own, DistT r2) {
+  int lo = 0, hi = tv.nv;
+  if (fm.warp_cloud && !fm.views) {
+    const int c = fm.warp_cloud[slot >> 5];
+    lo = (int)fm.valid_off[c];
+    hi = (int)fm.valid_off[c + 1];
+  }
+  top.seed(k, seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi), r2);
+}
+
 // order_mode 0: slot = query; 1: order[slot]; 2: tree order (query = the
 // original index stored at tree position slot).
 template <typename T, int D>
@@ -154,7 +210,7 @@ __global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
       c = box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], p) < box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], p);
     const int ref = nd.ref[c];
     if (ref < 0) {
-      k = -ref - 1;
+      k = -ref - 1 + nd.cnt[c] / 2;  // the middle of the leaf bucket
       break;
     }
     cur = ref;
@@ -199,31 +255,40 @@ __global__ void k_place(const int* key, int m, int* cursor, int* order) {
 
 // Builds a processing order in which queries near each other in the tree are
 // adjacent (counting sort on the tree position key).  Returns the order mode.
+//
+// For point queries `anchors` (m ints, optional) receives each query's leaf
+// start position (the seed anchor of the search), for every m.
 template <typename T, int D>
-int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaStream_t st, bool checked = false) {
+int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaStream_t st, bool checked = false,
+               int* anchors = nullptr) {
   if (!checked) check_indices(t, qs, st);
   Stage stage("order", st);
   const int m = (int)qs.m;
   const int nv = (int)t->nv;
   if (m <= 0) return 0;
   if (!qs.pts && !qs.idx && m == nv && t->n == t->nv) return 2;  // all points, tree order
-  if (m < 2048) return 0;
-  DevBuf<int> key(m, st), hist(nv + 2, st);
-  if (qs.pts) {
+  const bool locate = qs.pts && (anchors || m >= 2048);
+  DevBuf<int> keybuf((locate && anchors) || (!locate && m < 2048) ? 0 : m, st);
+  int* key = locate && anchors ? anchors : keybuf.get();
+  if (locate) {
     if (qs.qdtype == F64)
-      k_locate<T, D, double><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const double*)qs.pts, m, key.get());
+      k_locate<T, D, double><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const double*)qs.pts, m, key);
     else
-      k_locate<T, D, float><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const float*)qs.pts, m, key.get());
-  } else {
-    k_idxkey<<<div_up(m, 256), 256, 0, st>>>(qs.idx, t->fwd, m, nv, key.get());
+      k_locate<T, D, float><<<div_up(m, 256), 256, 0, st>>>(view_of<T, D>(t), (const float*)qs.pts, m, key);
+    PPTKG_CHECK_LAUNCH();
   }
-  PPTKG_CHECK_LAUNCH();
+  if (m < 2048) return 0;
+  DevBuf<int> hist(nv + 2, st);
+  if (!qs.pts) {
+    k_idxkey<<<div_up(m, 256), 256, 0, st>>>(qs.idx, t->fwd, m, nv, key);
+    PPTKG_CHECK_LAUNCH();
+  }
   PPTKG_CUDA(cudaMemsetAsync(hist.get(), 0, sizeof(int) * (nv + 2), st));
-  k_hist<<<div_up(m, 256), 256, 0, st>>>(key.get(), m, hist.get());
+  k_hist<<<div_up(m, 256), 256, 0, st>>>(key, m, hist.get());
   PPTKG_CHECK_LAUNCH();
   exclusive_scan<int, int>(hist.get(), hist.get(), nv + 1, (int*)nullptr, st);
   order.alloc(m, st);
-  k_place<<<div_up(m, 256), 256, 0, st>>>(key.get(), m, hist.get(), order.get());
+  k_place<<<div_up(m, 256), 256, 0, st>>>(key, m, hist.get(), order.get());
   PPTKG_CHECK_LAUNCH();
   return 1;
 }
@@ -232,27 +297,31 @@ int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaS
 template <typename T, int D, int KMAX, typename L>
 __global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
                                                   int k, typename DistOf<T>::type r2, int32_t* out_idx,
-                                                  int32_t* out_cnt, int* status, SlotMap fm) {
+                                                  int32_t* out_cnt, int* status, SlotMap fm, int lane_span) {
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
   WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
-  int qid = -1, own = -1;
+  int qid = -1, own = -1, anchor = -1;
   DistT q[D];
   bool active = false;
   if (fm.warp_cloud) {
     qid = forest_query(slot, fm, tv);
-    if (qid >= 0) active = ld.load(qid, tv, q, own);
+    if (qid >= 0) active = ld.load(qid, tv, q, own, &anchor);
   } else if (slot < m) {
     qid = query_of(slot, order, order_mode, tv);
-    active = ld.load(qid, tv, q, own);
+    active = ld.load(qid, tv, q, own, &anchor);
   }
   if (!active)
 #pragma unroll
     for (int d = 0; d < D; d++) q[d] = (DistT)0;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (!packet_knn<T, D>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (active) seed_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2);
+  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
+                      ? lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top)
+                      : packet_knn<T, D>(tv, q, own, active, r2, top, ws);
+  if (!ok) atomicExch(status, 1);
   if (qid >= 0) {
     int c = 0;
 #pragma unroll
@@ -275,7 +344,8 @@ void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int 
   if (smem > 48 * 1024)
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
-                                                                      d_idx, d_cnt, status, fm);
+                                                                      d_idx, d_cnt, status, fm,
+                                                                      g_tune_lane_span.load());
   PPTKG_CHECK_LAUNCH();
 }
 
@@ -319,17 +389,17 @@ void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32
   if (m <= 0) return;
   DevBuf<int> status(1, st);
   PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
-  DevBuf<int> order;
-  const int mode = make_order<T, D>(t, qs, order, st);
+  DevBuf<int> order, anchors(qs.pts ? m : 0, st);
+  const int mode = make_order<T, D>(t, qs, order, st, false, anchors.get());
   const DistT r2 = radius2<DistT>(dmax);
   Stage stage("knn", st);
   if (qs.pts) {
     if (qs.qdtype == F64)
-      dispatch_knn<T, D>(t, PointQueries<double, D>{(const double*)qs.pts}, order.get(), mode, m, k, r2, d_idx, d_cnt,
-                         status.get(), st);
+      dispatch_knn<T, D>(t, PointQueries<double, D>{(const double*)qs.pts, anchors.get()}, order.get(), mode, m, k,
+                         r2, d_idx, d_cnt, status.get(), st);
     else
-      dispatch_knn<T, D>(t, PointQueries<float, D>{(const float*)qs.pts}, order.get(), mode, m, k, r2, d_idx, d_cnt,
-                         status.get(), st);
+      dispatch_knn<T, D>(t, PointQueries<float, D>{(const float*)qs.pts, anchors.get()}, order.get(), mode, m, k, r2,
+                         d_idx, d_cnt, status.get(), st);
   } else if (qs.exclude_self) {
     dispatch_knn<T, D>(t, IndexQueries<D, true>{qs.idx, t->fwd}, order.get(), mode, m, k, r2, d_idx, d_cnt,
                        status.get(), st);
@@ -558,29 +628,33 @@ __global__ void __launch_bounds__(QTHREADS, normals_min_blocks(KMAX, sizeof(type
 k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
-                                                      int* fix, int* nfix, int* status, SlotMap fm) {
+                                                      int* fix, int* nfix, int* status, SlotMap fm, int lane_span) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
   WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
   const int lane = threadIdx.x & 31;
-  int qid = -1, own = -1, grp = 0;
+  int qid = -1, own = -1, grp = 0, anchor = -1;
   DistT q[3];
   bool active = false;
   if (fm.warp_cloud) {
     grp = fm.views ? fm.warp_cloud[slot >> 5] : 0;
     qid = forest_query(slot, fm, tv);
-    if (qid >= 0) active = ld.load(qid, tv, q, own);
+    if (qid >= 0) active = ld.load(qid, tv, q, own, &anchor);
   } else if (slot < m) {
     qid = query_of(slot, order, order_mode, tv);
-    active = ld.load(qid, tv, q, own);
+    active = ld.load(qid, tv, q, own, &anchor);
   }
   if (!active) q[0] = q[1] = q[2] = (DistT)0;
   int* lane_log = ws.log + lane;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (!packet_knn<T, 3>(tv, q, own, active, r2, top, ws)) atomicExch(status, 1);
+  if (active) seed_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2);
+  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
+                      ? lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top)
+                      : packet_knn<T, 3>(tv, q, own, active, r2, top, ws);
+  if (!ok) atomicExch(status, 1);
   if (qid < 0) return;
   if (!active) {
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
@@ -724,7 +798,8 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
-      view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm);
+      view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm,
+      g_tune_lane_span.load());
   PPTKG_CHECK_LAUNCH();
 }
 
@@ -951,7 +1026,7 @@ template <typename T, int D>
 struct MultiTables {
   DevBuf<TreeView<T, D>> views;
   DevBuf<int64_t> slot_off, row_off;
-  DevBuf<int> warp_tree, order;
+  DevBuf<int> warp_tree, order, anchor;
   bool ordered = false;
   int64_t n_slots = 0;
   int depth = 0, n_nodes = 0;
@@ -1033,22 +1108,25 @@ static void check_indices_multi(const TreeBase* const* trees, int ntrees, const 
 // queries are neighbours.  `spec(g)` gives the QuerySpec of group g.
 template <typename T, int D, typename Spec>
 void multi_order(const TreeBase* const* trees, int ntrees, const int64_t* rows, MultiTables<T, D>& mt, Spec spec,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool anchors = false) {
   const int64_t m_all = rows[ntrees];
   bool any = false;
   for (int g = 0; g < ntrees && !any; g++) any = rows[g + 1] - rows[g] >= 2048;
-  if (!any) return;
-  mt.order.alloc(m_all, st);
+  if (!any && !anchors) return;
+  if (anchors) mt.anchor.alloc(m_all, st);
+  if (any) mt.order.alloc(m_all, st);
   for (int g = 0; g < ntrees; g++) {
     const int64_t m = rows[g + 1] - rows[g];
     if (m <= 0) continue;
     DevBuf<int> local;
-    const int mode = make_order<T, D>(trees[g], spec(g), local, st, true);
-    k_order_rows<<<div_up(m, 256), 256, 0, st>>>(mode == 1 ? local.get() : nullptr, (int)m, (int)rows[g],
-                                                 mt.order.get() + rows[g]);
-    PPTKG_CHECK_LAUNCH();
+    const int mode = make_order<T, D>(trees[g], spec(g), local, st, true, anchors ? mt.anchor.get() + rows[g] : nullptr);
+    if (any) {
+      k_order_rows<<<div_up(m, 256), 256, 0, st>>>(mode == 1 ? local.get() : nullptr, (int)m, (int)rows[g],
+                                                   mt.order.get() + rows[g]);
+      PPTKG_CHECK_LAUNCH();
+    }
   }
-  mt.ordered = true;
+  mt.ordered = any;
 }
 
 template <typename T, int D>
@@ -1067,18 +1145,18 @@ void multi_knn(const TreeBase* const* trees, int ntrees, const void* d_q, int qd
     qs.qdtype = qdtype;
     qs.m = rows[g + 1] - rows[g];
     return qs;
-  }, st);
+  }, st, true);
   std::unique_ptr<TreeBase> bt(bounds_tree(mt.depth, mt.n_nodes));
   DevBuf<int> status(1, st);
   PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
   const DistT r2 = radius2<DistT>(dmax);
   Stage stage("multi.knn", st);
   if (qdtype == F64)
-    dispatch_knn<T, D>(bt.get(), PointQueries<double, D>{(const double*)d_q}, nullptr, 0, (int)mt.n_slots, k, r2,
-                       d_idx, d_cnt, status.get(), st, mt.map());
+    dispatch_knn<T, D>(bt.get(), PointQueries<double, D>{(const double*)d_q, mt.anchor.get()}, nullptr, 0,
+                       (int)mt.n_slots, k, r2, d_idx, d_cnt, status.get(), st, mt.map());
   else
-    dispatch_knn<T, D>(bt.get(), PointQueries<float, D>{(const float*)d_q}, nullptr, 0, (int)mt.n_slots, k, r2, d_idx,
-                       d_cnt, status.get(), st, mt.map());
+    dispatch_knn<T, D>(bt.get(), PointQueries<float, D>{(const float*)d_q, mt.anchor.get()}, nullptr, 0,
+                       (int)mt.n_slots, k, r2, d_idx, d_cnt, status.get(), st, mt.map());
   check_status(status.get(), st, "multi-tree knn");
 }
 
