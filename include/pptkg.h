@@ -229,7 +229,7 @@ PPTKG_API int64_t pptkg_launch_count(void);
  * pptk_b200/autotune.py).  Settings are process-wide and read at launch.
  *   "lane_span": a kNN / normals warp whose 32 queries span more than this
  *     many tree positions walks the tree per lane rather than as one packet
- *     (-1: always packets).  Default 512.
+ *     (-1: always packets).  Default 256.
  * Unknown names or out-of-range values: PPTKG_E_INVALID. */
 PPTKG_API int pptkg_tune_set(const char* name, int64_t value);
 PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);

@@ -354,10 +354,21 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
   DistT smd[LSTACK];
   int sp = 0;
   auto need = [&](DistT md) { return md < r2 && md <= top.worst(); };
+  // a bucket is read four points at a time so that the loads overlap; the
+  // offers then go in position order against the current bound, as one by one
   auto scan = [&](int begin, int count) {
-    for (int p = begin; p < begin + count; p++) {
-      const PointRec<T, D> pr = tv.pts[p];
-      const DistT d2 = point_dist2<T, DistT, D>(pr.c, q);
+    const int end = begin + count;
+    int p = begin;
+    for (; p + 4 <= end; p += 4) {
+      DistT d2[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) d2[j] = point_dist2<T, DistT, D>(tv.pts[p + j].c, q);
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (d2[j] <= top.worst() && d2[j] < r2 && p + j != own) top.offer(d2[j], p + j);
+    }
+    for (; p < end; p++) {
+      const DistT d2 = point_dist2<T, DistT, D>(tv.pts[p].c, q);
       if (d2 <= top.worst() && d2 < r2 && p != own) top.offer(d2, p);
     }
   };

@@ -11,7 +11,7 @@
 namespace pptkg {
 
 std::atomic<long long> g_launches{0};
-std::atomic<int> g_tune_lane_span{512};
+std::atomic<int> g_tune_lane_span{256};
 
 namespace {
 struct Pending {

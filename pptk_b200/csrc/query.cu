@@ -26,6 +26,7 @@ TreeView<T, D> view_of(const TreeBase* t) {
   v.n_nodes = t->n_tnodes;
   v.root = t->root_tnode_h.empty() ? 0 : t->root_tnode_h[0];
   v.fwd = t->fwd;
+  v.n_in = (int)t->n;
   return v;
 }
 
@@ -81,16 +82,25 @@ struct PointQueries {
 // Query i is the stored point with original index idx[i] (or i); EXCL drops
 // the point itself from its own result (KNearestNeighborsSelf,
 // kdtree-impl.h:931-948; RNearNeighborsSelf, :1028-1043).
+//
+// `bad` (optional): indices are checked against the tree's rows on the
+// device; an index outside [0, n) sets *bad = 4 and leaves the query empty.
 template <int D, bool EXCL>
 struct IndexQueries {
   const int* idx;
   const int* fwd;
+  int* bad = nullptr;
   template <typename T, typename DistT>
   __device__ __forceinline__ bool load(int i, const TreeView<T, D>& tv, DistT* out, int& own,
                                        int* anchor = nullptr) const {
     const int o = idx ? idx[i] : i;
-    const int p = (fwd ? fwd : tv.fwd)[o];
     own = -1;
+    if (anchor) *anchor = -1;
+    if (bad && (o < 0 || o >= tv.n_in)) {
+      atomicExch(bad, 4);
+      return false;
+    }
+    const int p = (fwd ? fwd : tv.fwd)[o];
     if (anchor) *anchor = p;
     if (p < 0) return false;  // the point was dropped (NaN/inf): no neighbours
     const PointRec<T, D> r = tv.pts[p];
@@ -236,21 +246,34 @@ static void check_indices(const TreeBase* t, const QuerySpec& qs, cudaStream_t s
   if (h) throw Error(E_RANGE, "query index outside of [0, n)");
 }
 
-__global__ void k_idxkey(const int* idx, const int* fwd, int m, int nv, int* key) {
+// Tree position of each index query (nv for dropped points and, when the
+// indices are unchecked, for indices outside [0, n)).
+__global__ void k_idxkey(const int* idx, const int* fwd, int m, int n, int nv, int* key) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const int p = fwd[idx ? idx[i] : i];
+  const int o = idx ? idx[i] : i;
+  const int p = o >= 0 && o < n ? fwd[o] : -1;
   key[i] = p < 0 ? nv : p;
 }
 
-__global__ void k_hist(const int* key, int m, int* hist) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m) atomicAdd(&hist[key[i]], 1);
+// Counting sort on key >> shift: queries of the same run of 2^shift tree
+// positions share a bin (their relative order within it is immaterial).
+// The shift grows as the queries thin out, keeping bins about as many as
+// queries.
+static int order_shift(int nv, int m) {
+  int s = 0;
+  while (s < 20 && ((int64_t)m << (s + 1)) <= (int64_t)nv) s++;
+  return s;
 }
 
-__global__ void k_place(const int* key, int m, int* cursor, int* order) {
+__global__ void k_hist(const int* key, int m, int shift, int* hist) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m) order[atomicAdd(&cursor[key[i]], 1)] = i;
+  if (i < m) atomicAdd(&hist[key[i] >> shift], 1);
+}
+
+__global__ void k_place(const int* key, int m, int shift, int* cursor, int* order) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) order[atomicAdd(&cursor[key[i] >> shift], 1)] = i;
 }
 
 // Builds a processing order in which queries near each other in the tree are
@@ -278,17 +301,19 @@ int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaS
     PPTKG_CHECK_LAUNCH();
   }
   if (m < 2048) return 0;
-  DevBuf<int> hist(nv + 2, st);
+  const int shift = order_shift(nv, m);
+  const int bins = (nv >> shift) + 1;
+  DevBuf<int> hist(bins + 1, st);
   if (!qs.pts) {
-    k_idxkey<<<div_up(m, 256), 256, 0, st>>>(qs.idx, t->fwd, m, nv, key);
+    k_idxkey<<<div_up(m, 256), 256, 0, st>>>(qs.idx, t->fwd, m, (int)t->n, nv, key);
     PPTKG_CHECK_LAUNCH();
   }
-  PPTKG_CUDA(cudaMemsetAsync(hist.get(), 0, sizeof(int) * (nv + 2), st));
-  k_hist<<<div_up(m, 256), 256, 0, st>>>(key, m, hist.get());
+  PPTKG_CUDA(cudaMemsetAsync(hist.get(), 0, sizeof(int) * (bins + 1), st));
+  k_hist<<<div_up(m, 256), 256, 0, st>>>(key, m, shift, hist.get());
   PPTKG_CHECK_LAUNCH();
-  exclusive_scan<int, int>(hist.get(), hist.get(), nv + 1, (int*)nullptr, st);
+  exclusive_scan<int, int>(hist.get(), hist.get(), bins, (int*)nullptr, st);
   order.alloc(m, st);
-  k_place<<<div_up(m, 256), 256, 0, st>>>(key, m, hist.get(), order.get());
+  k_place<<<div_up(m, 256), 256, 0, st>>>(key, m, shift, hist.get(), order.get());
   PPTKG_CHECK_LAUNCH();
   return 1;
 }
@@ -376,6 +401,7 @@ static void check_status(int* d_status, cudaStream_t st, const char* what) {
   int h = 0;
   PPTKG_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h == 4) throw Error(E_RANGE, std::string(what) + ": query index outside of its tree's [0, n)");
   if (h) throw Error(E_DEVICE, std::string(what) + ": device traversal check failed (code " + std::to_string(h) + ")");
 }
 
@@ -1021,18 +1047,20 @@ template void forest_normals<double>(const TreeBase*, int, float, int, int, doub
 
 // ---------------------------------------------------- multi-tree batches --
 // Device tables of a multi-tree batch: TreeViews, per-warp group, slot and
-// row offsets.  `rows` are host offsets (ntrees + 1) of each tree's queries.
+// row offsets, uploaded as one block.  `rows` are host offsets (ntrees + 1)
+// of each tree's queries.
 template <typename T, int D>
 struct MultiTables {
-  DevBuf<TreeView<T, D>> views;
-  DevBuf<int64_t> slot_off, row_off;
-  DevBuf<int> warp_tree, order, anchor;
+  DevBuf<char> blob;
+  const TreeView<T, D>* views = nullptr;
+  const int64_t *slot_off = nullptr, *row_off = nullptr;
+  const int* warp_tree = nullptr;
+  DevBuf<int> order, anchor;
   bool ordered = false;
   int64_t n_slots = 0;
   int depth = 0, n_nodes = 0;
   SlotMap map() const {
-    return SlotMap{warp_tree.get(), slot_off.get(), nullptr, nullptr, views.get(), row_off.get(),
-                   ordered ? order.get() : nullptr};
+    return SlotMap{warp_tree, slot_off, nullptr, nullptr, views, row_off, ordered ? order.get() : nullptr};
   }
 };
 
@@ -1056,19 +1084,25 @@ void multi_tables(const TreeBase* const* trees, int ntrees, const int64_t* rows,
   if (mt.n_slots > INT32_MAX) throw Error(E_INVALID, "batch too large for one pass");
   // every view uses the batch-wide stack bound (shared memory is sized once)
   for (auto& x : v) x.depth = mt.depth;
-  std::vector<int> wt(std::max<int64_t>(mt.n_slots / 32, 1), 0);
+  const size_t nw = (size_t)std::max<int64_t>(mt.n_slots / 32, 1);
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t o_views = 0, o_so = up(sizeof(TreeView<T, D>) * ntrees), o_ro = o_so + up(8 * (ntrees + 1)),
+               o_wt = o_ro + up(8 * (ntrees + 1)), total = o_wt + up(4 * nw);
+  std::vector<char> h(total, 0);
+  memcpy(h.data() + o_views, v.data(), sizeof(TreeView<T, D>) * ntrees);
+  memcpy(h.data() + o_so, so.data(), 8 * (ntrees + 1));
+  memcpy(h.data() + o_ro, rows, 8 * (ntrees + 1));
+  int* wt = reinterpret_cast<int*>(h.data() + o_wt);
   for (int g = 0; g < ntrees; g++)
     for (int64_t w = so[g] / 32; w < so[g + 1] / 32; w++) wt[w] = g;
-  mt.views.alloc(ntrees, st);
-  mt.slot_off.alloc(ntrees + 1, st);
-  mt.row_off.alloc(ntrees + 1, st);
-  mt.warp_tree.alloc(wt.size(), st);
-  PPTKG_CUDA(cudaMemcpyAsync(mt.views.get(), v.data(), sizeof(TreeView<T, D>) * ntrees, cudaMemcpyHostToDevice, st));
-  PPTKG_CUDA(cudaMemcpyAsync(mt.slot_off.get(), so.data(), sizeof(int64_t) * (ntrees + 1), cudaMemcpyHostToDevice, st));
-  PPTKG_CUDA(cudaMemcpyAsync(mt.row_off.get(), rows, sizeof(int64_t) * (ntrees + 1), cudaMemcpyHostToDevice, st));
-  PPTKG_CUDA(cudaMemcpyAsync(mt.warp_tree.get(), wt.data(), sizeof(int) * wt.size(), cudaMemcpyHostToDevice, st));
-  // the host vectors go out of scope: finish the copies first
-  PPTKG_CUDA(cudaStreamSynchronize(st));
+  mt.blob.alloc(total, st);
+  // pageable source: the call returns once the bytes are staged, so `h` may
+  // go out of scope without a synchronisation
+  PPTKG_CUDA(cudaMemcpyAsync(mt.blob.get(), h.data(), total, cudaMemcpyHostToDevice, st));
+  mt.views = reinterpret_cast<const TreeView<T, D>*>(mt.blob.get() + o_views);
+  mt.slot_off = reinterpret_cast<const int64_t*>(mt.blob.get() + o_so);
+  mt.row_off = reinterpret_cast<const int64_t*>(mt.blob.get() + o_ro);
+  mt.warp_tree = reinterpret_cast<const int*>(mt.blob.get() + o_wt);
 }
 
 // A stand-in tree carrying the batch-wide traversal bounds for the launch
@@ -1083,24 +1117,6 @@ static TreeBase* bounds_tree(int depth, int n_nodes) {
 __global__ void k_order_rows(const int* local, int m, int base, int* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) out[i] = base + (local ? local[i] : i);
-}
-
-// Rejects index queries outside their own tree's [0, n): one status word for
-// the whole batch, one synchronisation.
-static void check_indices_multi(const TreeBase* const* trees, int ntrees, const int32_t* d_idx, const int64_t* rows,
-                                cudaStream_t st) {
-  DevBuf<int> status(1, st);
-  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
-  for (int g = 0; g < ntrees; g++) {
-    const int64_t m = rows[g + 1] - rows[g];
-    if (m <= 0) continue;
-    k_check_idx<<<div_up(m, 256), 256, 0, st>>>(d_idx + rows[g], (int)m, (int)trees[g]->n, status.get());
-    PPTKG_CHECK_LAUNCH();
-  }
-  int h = 0;
-  PPTKG_CUDA(cudaMemcpyAsync(&h, status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
-  PPTKG_CUDA(cudaStreamSynchronize(st));
-  if (h) throw Error(E_RANGE, "query index outside of its tree's [0, n)");
 }
 
 // Processing order of a multi-tree batch: each tree's queries sorted by
@@ -1170,8 +1186,8 @@ void multi_normals(const TreeBase* const* trees, int ntrees, const int32_t* d_id
   MultiTables<T, 3> mt;
   multi_tables<T, 3>(trees, ntrees, rows, mt, st);
   if (mt.n_slots == 0) return;
-  // every query index must lie within its own tree's input rows
-  check_indices_multi(trees, ntrees, d_idx, rows, st);
+  // query indices are checked against their own tree's rows by the kernels
+  // (status 4); the ordering pass maps bad ones to the end of the order
   multi_order<T, 3>(trees, ntrees, rows, mt, [&](int g) {
     QuerySpec qs;
     qs.idx = d_idx + rows[g];
@@ -1187,8 +1203,8 @@ void multi_normals(const TreeBase* const* trees, int ntrees, const int32_t* d_id
   int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
   Stage stage("multi.normals", st);
   // fwd comes from each warp's TreeView (null here)
-  dispatch_normals<T, IndexQueries<3, false>>(bt.get(), IndexQueries<3, false>{d_idx, nullptr}, nullptr, 0,
-                                              (int)mt.n_slots, k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals,
+  dispatch_normals<T, IndexQueries<3, false>>(bt.get(), IndexQueries<3, false>{d_idx, nullptr, status.get()}, nullptr,
+                                              0, (int)mt.n_slots, k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals,
                                               d_sizes, status.get(), st, mt.map());
   check_status(status.get(), st, "multi-tree normals");
 }

@@ -62,6 +62,7 @@ struct TreeView {
   int32_t n_nodes;  // TNode count: no traversal visits more nodes than this
   int32_t root;     // TNode where this tree's traversals start
   const int32_t* fwd;  // original row -> tree position
+  int32_t n_in;        // original rows (entries of fwd)
 };
 
 // Host-side owner of one device tree, or of a forest of independent trees

@@ -16,7 +16,7 @@ import math
 import threading
 import time
 from collections import deque
-from concurrent.futures import Future
+from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
 
@@ -51,8 +51,11 @@ class GpuEngine:
         self.torch = torch
         self.device = torch.device("cuda", device)
 
-    def stream(self):
-        return self.torch.cuda.Stream(device=self.device)
+    def stream(self, high_priority=False):
+        """A CUDA stream of this device; high-priority streams get free SMs
+        first, so a small batch does not wait behind a large one."""
+        lo, hi = self.torch.cuda.Stream.priority_range()
+        return self.torch.cuda.Stream(device=self.device, priority=hi if high_priority else lo)
 
     def build(self, points, maxleafsize, emptysplit, stream):
         from . import kdtree
@@ -154,21 +157,28 @@ class Server:
 
     budget_bytes: HBM the server may commit to resident trees plus the
         transient needs of admitted requests.
-    slots: batches that may run at once, each on its own CUDA stream.
+    slots: batches that may run at once, each on its own CUDA stream; the
+        last `fast_slots` of them run on high-priority streams and take the
+        batches of at most `small_batch` queries first.
     max_batch_queries: upper bound on the queries folded into one batch.
     """
 
-    def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=8_000_000, engine=None):
+    def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=8_000_000, engine=None,
+                 fast_slots=1, small_batch=1_000_000):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)
         self.max_batch = int(max_batch_queries)
+        self.small_batch = int(small_batch)
         self.trees = {}
         self.tree_bytes = {}
         self._next_id = 0
         self._pending = deque()
         self._committed = 0.0
         self._cv = threading.Condition()
-        self._free = [self.engine.stream() for _ in range(slots)]
+        fast_slots = max(0, min(int(fast_slots), slots - 1))
+        self._free = [(self.engine.stream(False), False) for _ in range(slots - fast_slots)]
+        self._free += [(self.engine.stream(True), True) for _ in range(fast_slots)]
+        self._pool = ThreadPoolExecutor(max_workers=slots, thread_name_prefix="pptk-b200-slot")
         self._running = True
         self._done = []
         self._batches = 0
@@ -264,11 +274,14 @@ class Server:
                 if not batch:
                     self._cv.wait(0.001)
                     continue
-                stream = self._free.pop()
+                small = sum(r.m for r in batch) <= self.small_batch
+                pick = next((i for i, (_, fast) in enumerate(self._free) if fast == small), len(self._free) - 1)
+                slot = self._free.pop(pick)
                 self._batches += 1
-            threading.Thread(target=self._run, args=(batch, stream), daemon=True).start()
+            self._pool.submit(self._run, batch, slot)
 
-    def _run(self, batch, stream):
+    def _run(self, batch, slot):
+        stream = slot[0]
         t0 = time.perf_counter()
         for r in batch:
             r.t_start = t0
@@ -310,7 +323,7 @@ class Server:
             with self._cv:
                 for r in batch:
                     self._committed -= r.bytes
-                self._free.append(stream)
+                self._free.append(slot)
                 self._cv.notify_all()
 
     def _finish(self, rs, results, stream):
@@ -344,3 +357,4 @@ class Server:
             self._running = False
             self._cv.notify_all()
         self._thread.join(timeout=30)
+        self._pool.shutdown(wait=True)

@@ -103,3 +103,23 @@ def test_server_answers_are_the_same_alone_and_in_the_mix(gpu):
             assert torch.is_tensor(got) == on_device
             assert np.array_equal(_np(got), _np(alone))
     srv.close()
+
+
+def test_multi_tree_normals_rejects_an_index_outside_its_tree(gpu):
+    from pptk_b200 import _native as N
+    clouds, trees, _ = trees_and_queries(gpu, seed=4)
+    ids = [np.arange(min(len(c), 100), dtype=np.int32) for c in clouds]
+    ids[1] = np.array([0, 1, 3], np.int32)  # the second tree holds 3 points: row 3 is outside
+    rows = np.concatenate([[0], np.cumsum([len(i) for i in ids])]).astype(np.int64)
+    I = np.ascontiguousarray(np.concatenate(ids))
+    ev = np.empty((len(I), 3), np.float32)
+    handles = (ctypes.c_void_p * len(trees))(*[t._h.value for t in trees])
+    with pytest.raises(RuntimeError, match="outside"):
+        N.call("pptkg_multi_normals", handles, len(trees), N.ptr(I), N.ptr(rows), N.MEM_HOST, 10,
+               ctypes.c_float(np.inf), 1, 0, N.ptr(ev), None, None, None)
+    # the library stays usable after the error
+    ids[1] = np.array([0, 1, 2], np.int32)
+    I = np.ascontiguousarray(np.concatenate(ids))
+    N.call("pptkg_multi_normals", handles, len(trees), N.ptr(I), N.ptr(rows), N.MEM_HOST, 10,
+           ctypes.c_float(np.inf), 1, 0, N.ptr(ev), None, None, None)
+    assert np.isfinite(ev).all()

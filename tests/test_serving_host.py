@@ -24,7 +24,7 @@ class FakeEngine:
         self.batches = []
         self.lock = threading.Lock()
 
-    def stream(self):
+    def stream(self, high_priority=False):
         return object()
 
     def build(self, points, maxleafsize, emptysplit, stream):
