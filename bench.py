@@ -28,6 +28,11 @@ the whole stream (40M queries).
 * ``cpu_baseline``: the reference's own k-d tree (compiled from its sources
   in oracle/_ref) with the restated normal loop, on a bounded sample, using
   every host core.
+* ``precision``: angular error (p50/p99/max, radians) of the FP32 normal
+  path against FP64 on three clouds (200k uniform float32 k=16, the 20M
+  scene k=16, 10M float64 planar patches offset 1e5 m k=24): all rows
+  against the device FP64 path, and 20k sampled rows against the CPU FP64
+  oracle (float64 covariance of the oracle's own neighbours).
 
 ``--workload plain`` times one drop-in ``estimate_normals`` over all 20M
 points instead (device build + fused kNN+PCA).  ``--impl reference`` times
@@ -69,6 +74,7 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=1_000_000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 angular error report")
     return p.parse_args()
 
 
@@ -199,17 +205,23 @@ def run_reference(args):
 
 
 class Ctx:
-    """Per-rank plumbing: device, barrier, max over ranks, native library."""
+    """Per-rank plumbing: device, barrier, max over ranks, native library.
+    Every rank is an independent replica; the only collectives are the
+    barriers around the timed region and the max of the per-rank times.
+    backend/device default to NCCL on this rank's GPU (gloo/cpu for tests
+    of the replica logic)."""
 
-    def __init__(self):
+    def __init__(self, backend="nccl", device=None):
         import torch
         self.torch = torch
         self.world, self.rank, self.local = dist_env()
-        torch.cuda.set_device(self.local)
+        self.device = device or f"cuda:{self.local}"
+        if self.device.startswith("cuda"):
+            torch.cuda.set_device(self.local)
         if self.world > 1:
             import torch.distributed as dist
             from datetime import timedelta
-            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+            dist.init_process_group(backend, timeout=timedelta(seconds=300))
         from pptk_b200 import _native as N
         self.N = N
         self.lib = N.lib()
@@ -220,11 +232,15 @@ class Ctx:
             dist.barrier()
 
     def max_over_ranks(self, x):
-        t = self.torch.tensor([float(x)], device="cuda")
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
         if self.world > 1:
             import torch.distributed as dist
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    def throughput(self, units_per_rank, seconds):
+        """Whole-job rate: every rank's units over the slowest rank's time."""
+        return self.world * units_per_rank / self.max_over_ranks(seconds)
 
     def stage(self, name):
         t, c = ctypes.c_double(), ctypes.c_int64()
@@ -301,7 +317,7 @@ def run_plain_workload(args, ctx):
     roof = roofline(ctx, "normals", n * args.steps)
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
-    value = ctx.world * n / (ms_max / 1e3)
+    value = ctx.throughput(n, ms / 1e3)
     e2e = None
     if not args.no_e2e:
         host = torch.from_numpy(pts).pin_memory().numpy()
@@ -373,7 +389,7 @@ def run_serving_workload(args, ctx):
     roof = roofline(ctx, "multi.normals", n_norm * args.steps)
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
-    value = ctx.world * per_step / (ms_max / 1e3)
+    value = ctx.throughput(per_step, ms / 1e3)
 
     # latency at a fixed offered load: Poisson arrivals at half the measured
     # serving throughput, requests drawn in stream order
@@ -475,11 +491,66 @@ def run_serving_workload(args, ctx):
             "clocks": clk}
 
 
+def angle_stats(a, b):
+    """p50/p99/max of the unsigned angle (rad) between row vectors of two
+    CUDA tensors, over rows finite in both."""
+    import torch
+    a = a.double()
+    b = b.double()
+    ok = torch.isfinite(a).all(1) & torch.isfinite(b).all(1)
+    a, b = a[ok], b[ok]
+    cr = torch.linalg.norm(torch.cross(a, b, dim=1), dim=1)
+    dt = (a * b).sum(1).abs()
+    ang = torch.sort(torch.atan2(cr, dt)).values
+    n = ang.numel()
+    if n == 0:
+        return {"p50": None, "p99": None, "max": None, "rows": 0}
+    return {"p50": float(ang[int(0.5 * (n - 1))]), "p99": float(ang[int(0.99 * (n - 1))]), "max": float(ang[-1]),
+            "rows": int(n)}
+
+
+def precision_report():
+    """FP32 normal path against FP64 on the configs' clouds: every row
+    against the device FP64 path, and a sample of rows against the CPU FP64
+    oracle (float64 covariance of the same neighbours, numpy eigh)."""
+    import torch
+    from oracle import oracle as O
+    from pptk_b200 import estimate_normals, synth
+    out = {}
+    cases = [("uniform_200k_f32_k16", lambda: synth.uniform_cube(200_000, seed=0), 16, "auto"),
+             ("lidar_scene_20M_f32_k16", lambda: synth.lidar_scene(20_000_000, seed=2), 16, "auto"),
+             ("planar_patches_10M_f64_k24", lambda: synth.planar_patches(10_000_000, seed=3)[0], 24, "fp32")]
+    for name, gen, k, prec in cases:
+        P = gen()
+        dev = torch.from_numpy(P).cuda()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n32 = estimate_normals(dev, k, np.inf, precision=prec, verbose=False)
+        torch.cuda.synchronize()
+        t32 = time.perf_counter() - t0
+        n64 = estimate_normals(dev, k, np.inf, precision="fp64", verbose=False)
+        rows = np.sort(np.random.default_rng(5).choice(len(P), size=min(20_000, len(P)), replace=False)).astype(
+            np.int32)
+        _, _, _, nb = O.port_estimate_normals(P, k, np.inf, subsample=rows, num_eigen=3, want_nbrs=True)
+        w, V, _ = O.normals_fp64(P, nb)
+        ref = torch.from_numpy(np.ascontiguousarray(V[:, 0, :])).cuda()
+        out[name] = {"dtype": str(P.dtype), "k": k, "fp32_path": prec,
+                     "fp32_path_queries_per_s": len(P) / t32,
+                     "vs_device_fp64_all_rows": angle_stats(n32, n64),
+                     "vs_cpu_fp64_oracle_sample": angle_stats(n32[torch.from_numpy(rows).cuda().long()], ref),
+                     "device_fp64_vs_cpu_fp64_oracle_sample": angle_stats(
+                         n64[torch.from_numpy(rows).cuda().long()], ref)}
+        del dev, n32, n64
+    return out
+
+
 def run_ours(args):
     ctx = Ctx()
     ctx.lib.pptkg_profile_enable.argtypes = [ctypes.c_int]
     ctx.lib.pptkg_launch_count.restype = ctypes.c_int64
     res = (run_serving_workload if args.workload == "serving" else run_plain_workload)(args, ctx)
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_precision:
+        res["precision"] = precision_report()
     if ctx.rank == 0:
         line = {"metric": METRIC, "value": res.pop("value"), "unit": "queries/s", "n_gpus": ctx.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
