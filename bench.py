@@ -64,7 +64,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="serving", choices=["serving", "plain"])
+    p.add_argument("--workload", default="serving", choices=["serving", "plain", "ragged"])
     p.add_argument("--points", type=int, default=20_000_000)
     p.add_argument("--k", type=int, default=16)
     p.add_argument("--slots", type=int, default=3)
@@ -342,6 +342,77 @@ def run_plain_workload(args, ctx):
             "clocks": clk}
 
 
+def run_ragged_workload(args, ctx):
+    """Ragged batch: 4,096 clouds (synth.ragged_clouds, seed 4, sizes
+    log-uniform in [1k, 200k]); one step builds every cloud's tree in one
+    forest build and answers kNN k=16 and normals k=16 for every point of
+    every cloud.  Bucket size and lane_span are picked by the autotuner on
+    the first 256 clouds before timing."""
+    torch = ctx.torch
+    from pptk_b200 import autotune, ragged, synth
+    k = args.k
+    P, off = synth.ragged_clouds(4096, seed=4)
+    n = len(P)
+    dev = torch.from_numpy(P).cuda()
+    sample_end = int(off[256])
+    fs = ragged.Forest(dev[:sample_end], off[:257])
+    tuned = autotune.tune(lambda: (fs.knn(k), fs.normals(k)), fs.set_bucket)
+    del fs
+
+    def step():
+        f = ragged.Forest(dev, off)
+        f.set_bucket(tuned["bucket"])
+        f.knn(k)
+        f.normals(k)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.lib.pptkg_profile_enable(1)
+    ms, launches, clk = device_timed(ctx, step, args.steps)
+    stages = {}
+    for nm in ("build", "build.levels", "build.subtree", "forest.knn", "forest.normals"):
+        t_, c_ = ctx.stage(nm)
+        stages[nm] = t_ / max(c_, 1) if c_ else 0.0
+    roof = roofline(ctx, "forest.normals", n * args.steps)
+    ctx.lib.pptkg_profile_enable(0)
+    ms_max = ctx.max_over_ranks(ms)
+    value = ctx.throughput(n, ms / 1e3)
+    # the same queries replayed from CUDA graphs on a built forest
+    f = ragged.Forest(dev, off)
+    f.set_bucket(tuned["bucket"])
+    cap_k, _ = f.capture_knn(k)
+    cap_n, _ = f.capture_normals(k)
+    ms_q, _, _ = device_timed(ctx, lambda: (cap_k.replay(), cap_n.replay()), args.steps)
+    cap_k.check()
+    cap_n.check()
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(P).pin_memory().numpy()
+        ctx.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fh = ragged.Forest(host, off)
+            fh.set_bucket(tuned["bucket"])
+            i, c = fh.knn(k)
+            nn = fh.normals(k)
+        dt = ctx.max_over_ranks((time.perf_counter() - t0) / args.steps)
+        e2e = {"value": ctx.world * n / dt, "unit": "queries/s", "h2d_bytes_per_step": int(P.nbytes),
+               "d2h_bytes_per_step": int(i.nbytes + c.nbytes + nn.nbytes)}
+    return {"value": value, "ms_per_step": ms_max,
+            "config": {"workload": f"ragged batch of 4096 float32 clouds ({n} points, sizes log-uniform in "
+                                   f"[1k, 200k]): forest build + kNN k={k} + normals k={k} for every point",
+                       "clouds": 4096, "points": n, "k": k, "l2": f"inputs ({P.nbytes / 1e9:.2f} GB) larger than L2",
+                       "parallelism": f"replicas x{ctx.world}"},
+            "autotune": {"bucket": tuned["bucket"], "lane_span": tuned["lane_span"],
+                         "sample": "first 256 clouds", "table": tuned["table"]},
+            "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
+                             "ms_per_step": ms_q, "what": "kNN + normals of every point, replayed from two CUDA "
+                                                         "graphs on the built forest"},
+            "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof,
+            "cpu_baseline": None, "clocks": clk}
+
+
 def percentiles(lat_s):
     a = np.asarray(lat_s, dtype=np.float64) * 1e3
     return {"p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)), "requests": int(a.size)}
@@ -548,7 +619,8 @@ def run_ours(args):
     ctx = Ctx()
     ctx.lib.pptkg_profile_enable.argtypes = [ctypes.c_int]
     ctx.lib.pptkg_launch_count.restype = ctypes.c_int64
-    res = (run_serving_workload if args.workload == "serving" else run_plain_workload)(args, ctx)
+    res = {"serving": run_serving_workload, "plain": run_plain_workload,
+           "ragged": run_ragged_workload}[args.workload](args, ctx)
     if ctx.rank == 0 and ctx.world == 1 and not args.no_precision:
         res["precision"] = precision_report()
     if ctx.rank == 0:

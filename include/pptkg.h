@@ -234,6 +234,15 @@ PPTKG_API int64_t pptkg_launch_count(void);
 PPTKG_API int pptkg_tune_set(const char* name, int64_t value);
 PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);
 
+/* Status sink of the calling host thread (no reference counterpart; for
+ * capturing forest queries into a CUDA graph).  While d_word (a device int,
+ * or NULL to clear) is set, pptkg_forest_knn / pptkg_forest_normals with
+ * device buffers record kernel check failures by writing a non-zero code
+ * into *d_word and neither synchronise nor read it back; the caller zeroes
+ * the word and checks it after the work (or a graph replay) completes.  A
+ * forest's first query sets up device tables and must run without a sink. */
+PPTKG_API int pptkg_set_status_sink(int* d_word);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,7 @@ SIGNATURES = {
     "pptkg_profile_get": [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), _pi64],
     "pptkg_tune_set": [ctypes.c_char_p, _i64],
     "pptkg_tune_get": [ctypes.c_char_p, _pi64],
+    "pptkg_set_status_sink": [_vp],
 }
 
 _lib = None

@@ -305,7 +305,7 @@ int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int exclude_s
       forest_knn<T, Dm>(t, k, dmax, exclude_self != 0, oi.d, oc.d, S(stream));
       oi.flush(S(stream));
       oc.flush(S(stream));
-      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+      if (!(g_status_sink && mem == PPTKG_MEM_DEVICE)) PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
     });
   });
 }
@@ -326,7 +326,7 @@ int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen
       ev.flush(S(stream));
       ew.flush(S(stream));
       sz.flush(S(stream));
-      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+      if (!(g_status_sink && mem == PPTKG_MEM_DEVICE)) PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
     });
   });
 }

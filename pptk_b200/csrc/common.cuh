@@ -45,6 +45,12 @@ extern std::atomic<long long> g_launches;
 //  lane_span: a kNN warp whose queries span more than this many tree
 //    positions walks the tree per lane instead of as a packet (-1: never).
 extern std::atomic<int> g_tune_lane_span;
+
+// Status sink of this host thread (pptkg_set_status_sink): while set, query
+// entry points record kernel check failures into this device word and
+// neither synchronise nor read it back, so their launches can be captured
+// into a CUDA graph.
+extern thread_local int* g_status_sink;
 #define PPTKG_CHECK_LAUNCH()          \
   do {                                \
     ::pptkg::g_launches++;            \

@@ -12,6 +12,7 @@ namespace pptkg {
 
 std::atomic<long long> g_launches{0};
 std::atomic<int> g_tune_lane_span{256};
+thread_local int* g_status_sink = nullptr;
 
 namespace {
 struct Pending {
@@ -93,6 +94,11 @@ int pptkg_tune_set(const char* name, int64_t value) {
     return PPTKG_OK;
   }
   return PPTKG_E_INVALID;
+}
+
+int pptkg_set_status_sink(int* d_word) {
+  pptkg::g_status_sink = d_word;
+  return PPTKG_OK;
 }
 
 int pptkg_tune_get(const char* name, int64_t* value) {

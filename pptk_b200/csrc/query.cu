@@ -397,12 +397,34 @@ DistT radius2(double dmax) {
   return r * r;
 }
 
+// The status word of one query call: the thread's status sink when one is
+// set (nothing is read back), else a fresh zeroed word checked at the end.
+struct StatusWord {
+  DevBuf<int> own;
+  int* p = nullptr;
+  explicit StatusWord(cudaStream_t st) {
+    if (g_status_sink) {
+      p = g_status_sink;
+    } else {
+      own.alloc(1, st);
+      PPTKG_CUDA(cudaMemsetAsync(own.get(), 0, sizeof(int), st));
+      p = own.get();
+    }
+  }
+  int* get() const { return p; }
+  void check(cudaStream_t st, const char* what);
+};
+
 static void check_status(int* d_status, cudaStream_t st, const char* what) {
   int h = 0;
   PPTKG_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   PPTKG_CUDA(cudaStreamSynchronize(st));
   if (h == 4) throw Error(E_RANGE, std::string(what) + ": query index outside of its tree's [0, n)");
   if (h) throw Error(E_DEVICE, std::string(what) + ": device traversal check failed (code " + std::to_string(h) + ")");
+}
+
+void StatusWord::check(cudaStream_t st, const char* what) {
+  if (!g_status_sink) check_status(p, st, what);
 }
 
 template <typename T, int D>
@@ -959,6 +981,8 @@ __global__ void k_warp_cloud(const int64_t* slot_off, int ncloud, int64_t nwarps
 // slots [slot_off[c], slot_off[c] + count), rounded up to whole warps.
 static SlotMap slot_map(const TreeBase* t, int64_t& n_slots, cudaStream_t st) {
   TreeBase* mt = const_cast<TreeBase*>(t);
+  if (!mt->warp_cloud && g_status_sink)
+    throw Error(E_INVALID, "a forest's first query must run without a status sink (it synchronises once)");
   if (!mt->warp_cloud) {
     std::vector<int64_t> so(t->ncloud + 1, 0);
     for (int c = 0; c < t->ncloud; c++) {
@@ -993,8 +1017,7 @@ void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_
   PPTKG_CUDA(cudaMemsetAsync(d_idx, 0xff, sizeof(int32_t) * (size_t)t->n * k, st));
   if (d_cnt) PPTKG_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)t->n, st));
   if (n_slots == 0) return;
-  DevBuf<int> status(1, st);
-  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  StatusWord status(st);
   const DistT r2 = radius2<DistT>(dmax);
   Stage stage("forest.knn", st);
   if (exclude_self)
@@ -1003,7 +1026,7 @@ void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_
   else
     dispatch_knn<T, D>(t, IndexQueries<D, false>{nullptr, t->fwd}, nullptr, 0, (int)n_slots, k, r2, d_idx, d_cnt,
                        status.get(), st, fm);
-  check_status(status.get(), st, "forest knn");
+  status.check(st, "forest knn");
 }
 
 template <typename T>
@@ -1026,8 +1049,7 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
     PPTKG_CHECK_LAUNCH();
   }
   if (n_slots == 0) return;
-  DevBuf<int> status(1, st);
-  PPTKG_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+  StatusWord status(st);
   const DistT rr = (DistT)(T)r;
   const DistT r2 = rr * rr;
   int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
@@ -1035,7 +1057,7 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
   dispatch_normals<T, IndexQueries<3, false>>(t, IndexQueries<3, false>{nullptr, t->fwd}, nullptr, 0, (int)n_slots,
                                               k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals, d_sizes, status.get(),
                                               st, fm);
-  check_status(status.get(), st, "forest normals");
+  status.check(st, "forest normals");
 }
 
 template void forest_knn<float, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);

@@ -118,3 +118,71 @@ class Forest:
         if ew is None and sz is None:
             return ev
         return ev, ew, sz
+
+    # ------------------------------------------------------ graph capture --
+    def _capture(self, issue):
+        """Captures issue(stream) -- one native forest query into fixed output
+        tensors -- into a CUDA graph.  The query runs once uncaptured first
+        (it sets up the forest's slot tables and loads the kernels)."""
+        import torch
+        if not self._torch:
+            raise ValueError("graph capture needs a forest built from CUDA tensors")
+        sink = torch.zeros(1, dtype=torch.int32, device=self.device)
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            issue(N.torch_stream(self.device))
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            N.call("pptkg_set_status_sink", N.ptr(sink))
+            try:
+                issue(N.torch_stream(self.device))
+            finally:
+                N.call("pptkg_set_status_sink", None)
+        return CapturedQuery(g, sink)
+
+    def capture_knn(self, k, dmax=math.inf, exclude_self=True):
+        """(CapturedQuery, (indices, counts)): Forest.knn captured into a CUDA
+        graph; every replay() rewrites the two tensors."""
+        idx = self._new((self.n, int(k)), np.int32)
+        cnt = self._new((self.n,), np.int32)
+
+        def issue(stream):
+            N.call("pptkg_forest_knn", self._h, int(k), float(np.float32(dmax)), int(bool(exclude_self)), self._mem,
+                   N.ptr(idx), N.ptr(cnt), stream, where="Forest.capture_knn()")
+
+        return self._capture(issue), (idx, cnt)
+
+    def capture_normals(self, k, r=math.inf, precision="auto"):
+        """(CapturedQuery, normals): Forest.normals captured into a CUDA
+        graph."""
+        from .estimate_normals import PRECISIONS
+        if self.dim != 3:
+            raise TypeError("normals need 3-d points")
+        ev = self._new((self.n, 3), self.dtype)
+
+        def issue(stream):
+            N.call("pptkg_forest_normals", self._h, int(k), ctypes.c_float(float(np.float32(r))), 1,
+                   PRECISIONS[precision], self._mem, N.ptr(ev), None, None, stream, where="Forest.capture_normals()")
+
+        return self._capture(issue), ev
+
+
+class CapturedQuery:
+    """A forest query captured into a CUDA graph.  replay() launches it on
+    the current stream; check() waits for it and raises if a kernel check
+    failed in any replay since the last check."""
+
+    def __init__(self, graph, sink):
+        self.graph = graph
+        self.sink = sink
+
+    def replay(self):
+        self.graph.replay()
+
+    def check(self):
+        code = int(self.sink.item())
+        if code:
+            self.sink.zero_()
+            raise RuntimeError(f"captured forest query: device check failed (code {code})")

@@ -83,3 +83,54 @@ def test_ragged_config_shape_at_scale(gpu, port):
         cl = P[off[c]:off[c + 1]]
         oi, oc = port.PortTree(cl).knn_self(np.arange(len(cl), dtype=np.int32), 16)
         assert np.array_equal(idx[off[c]:off[c + 1]] - off[c], oi)
+
+
+def test_captured_forest_queries_replay(gpu):
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=5, count=20)
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    cap, (idx, cnt) = f.capture_knn(8)
+    ref_i, ref_c = f.knn(8)
+    for _ in range(2):
+        idx.fill_(-7)
+        cnt.fill_(-7)
+        cap.replay()
+        torch.cuda.synchronize()
+        cap.check()
+        assert torch.equal(idx, ref_i) and torch.equal(cnt, ref_c)
+    capn, ev = f.capture_normals(8)
+    ref_n = f.normals(8)
+    ev.fill_(5.0)
+    capn.replay()
+    capn.check()
+    assert torch.equal(torch.nan_to_num(ev, nan=-9.0), torch.nan_to_num(ref_n, nan=-9.0))
+
+
+def test_capture_needs_device_forest(gpu):
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=5, count=12)
+    with pytest.raises(ValueError):
+        ragged.Forest(P, off).capture_knn(4)
+
+
+def test_autotuned_settings_give_identical_results(gpu):
+    import torch
+    from pptk_b200 import _native as N
+    from pptk_b200 import autotune, ragged
+    P, off, _ = small_batch(seed=6, count=30)
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    ref_i, ref_c = f.knn(8)
+    ref_n = f.normals(8)
+    try:
+        res = autotune.tune(lambda: f.knn(8), f.set_bucket, buckets=(16, 64), lane_spans=(-1, 0), repeats=1)
+        assert res["bucket"] in (16, 64) and res["lane_span"] in (-1, 0) and len(res["table"]) == 4
+        for b, ls in ((16, -1), (64, 0), (res["bucket"], res["lane_span"])):
+            f.set_bucket(b)
+            N.tune_set("lane_span", ls)
+            i, c = f.knn(8)
+            assert torch.equal(i, ref_i) and torch.equal(c, ref_c), (b, ls)
+            n = f.normals(8)
+            assert torch.equal(torch.nan_to_num(n, nan=-9.0), torch.nan_to_num(ref_n, nan=-9.0)), (b, ls)
+    finally:
+        N.tune_set("lane_span", 256)
