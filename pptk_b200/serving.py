@@ -28,6 +28,24 @@ BUILD_SCRATCH_PER_POINT = 160
 QUERY_BYTES = 96
 
 
+def _kclass(k):
+    """Top-k capacity class of k (the kernels' compile-time capacities)."""
+    for c in (4, 8, 16, 32, 64):
+        if k <= c:
+            return c
+    return k
+
+
+def _first_k(idx, cnt, k, k_launch):
+    """The result of a k-query taken from a k_launch-query (k <= k_launch):
+    the first k columns and the counts capped at k."""
+    if k == k_launch:
+        return idx, cnt
+    if isinstance(cnt, np.ndarray):
+        return idx[:, :k], np.minimum(cnt, k)
+    return idx[:, :k], cnt.clamp(max=k)
+
+
 class Request:
     __slots__ = ("kind", "args", "future", "t_submit", "t_start", "t_done", "bytes", "m", "key")
 
@@ -199,8 +217,14 @@ class Server:
         m = int(queries.shape[0])
         dt = str(getattr(queries, "dtype", "float64"))
         host = isinstance(queries, np.ndarray) if to_host is None else bool(to_host)
-        r = Request("knn", (tree_id, queries), m * (QUERY_BYTES + 4 * int(k)), m,
-                    key=("knn", int(k), float(dmax), dt, host))
+        k = int(k)
+        if k < 1:
+            raise ValueError("k must be positive")
+        # requests whose k share a top-k capacity class run as one launch at
+        # the class's largest k; each gets its first k columns (the exact
+        # top-k of its own query)
+        r = Request("knn", (tree_id, queries, k), m * (QUERY_BYTES + 4 * _kclass(k)), m,
+                    key=("knn", _kclass(k), float(dmax), dt, host))
         return self._submit(r)
 
     def normals(self, tree_id, indices=None, k=16, r=math.inf, precision="auto", to_host=None):
@@ -303,8 +327,9 @@ class Server:
                     self._finish([r], [tid], stream)
                 elif kind == "knn":
                     trees = [self.trees[r.args[0]] for r in rs]
-                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], key[1], key[2], stream,
-                                                host=key[4])
+                    kl = max(r.args[2] for r in rs)
+                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], kl, key[2], stream, host=key[4])
+                    res = [_first_k(i, c, r.args[2], kl) for (i, c), r in zip(res, rs)]
                     self._finish(rs, res, stream)
                 elif kind == "normals":
                     trees = [self.trees[r.args[0]] for r in rs]
@@ -353,8 +378,14 @@ class Server:
         return out
 
     def close(self):
+        """Stops admitting work: requests still queued fail with
+        RuntimeError, running batches finish."""
         with self._cv:
             self._running = False
+            while self._pending:
+                r = self._pending.popleft()
+                if not r.future.done():
+                    r.future.set_exception(RuntimeError("server closed"))
             self._cv.notify_all()
-        self._thread.join(timeout=30)
+        self._thread.join()
         self._pool.shutdown(wait=True)

@@ -123,3 +123,21 @@ def test_multi_tree_normals_rejects_an_index_outside_its_tree(gpu):
     N.call("pptkg_multi_normals", handles, len(trees), N.ptr(I), N.ptr(rows), N.MEM_HOST, 10,
            ctypes.c_float(np.inf), 1, 0, N.ptr(ev), None, None, None)
     assert np.isfinite(ev).all()
+
+
+def test_server_merges_knn_requests_of_one_k_class(gpu):
+    from pptk_b200 import serving
+    rng = np.random.default_rng(8)
+    cloud = rng.random((200_000, 3), dtype=np.float32)
+    srv = serving.Server(budget_bytes=8e9, slots=1)
+    tid = srv.build(cloud).result(timeout=120)
+    blocker = srv.normals(tid, None, k=32)  # keeps the only slot busy while the others queue
+    qs = {5: cloud[:3000] + np.float32(1e-3), 7: cloud[5000:6000] - np.float32(1e-3), 20: cloud[9000:9100]}
+    futs = {k: srv.knn(tid, q, k=k) for k, q in qs.items()}
+    blocker.result(timeout=120)
+    tree = srv.trees[tid]
+    for k, q in qs.items():
+        idx, cnt = futs[k].result(timeout=120)
+        di, dc = gpu.kdtree.knn(tree, q, k)
+        assert np.array_equal(idx, di) and np.array_equal(cnt, dc), k
+    srv.close()

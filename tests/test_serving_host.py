@@ -33,7 +33,7 @@ class FakeEngine:
 
     def knn_batch(self, trees, queries, k, dmax, stream, host=False):
         with self.lock:
-            self.batches.append(("knn", len(trees)))
+            self.batches.append(("knn", len(trees), k))
         time.sleep(self.delay)
         out = []
         for t, q in zip(trees, queries):
@@ -99,4 +99,26 @@ def test_fifo_order_is_kept_across_kinds():
     f3 = srv.normals(tid, None, k=4)
     f1.result(timeout=10), f2.result(timeout=10), f3.result(timeout=10)
     assert f3.result().shape == (50, 3)
+    srv.close()
+
+
+def test_knn_requests_of_one_k_class_share_a_launch():
+    eng = FakeEngine(delay=0.05)
+    srv = serving.Server(budget_bytes=1e9, slots=1, engine=eng)
+    rng = np.random.default_rng(1)
+    pts = rng.random((300, 3))
+    tid = srv.build(pts).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((4, 3)), k=3)  # holds the only slot for a while
+    qs = {5: rng.random((6, 3)), 7: rng.random((5, 3)), 20: rng.random((3, 3))}
+    futs = {k: srv.knn(tid, q, k=k) for k, q in qs.items()}
+    blocker.result(timeout=10)
+    for k, q in qs.items():
+        idx, cnt = futs[k].result(timeout=10)
+        d = ((q[:, None, :] - pts[None]) ** 2).sum(-1)
+        assert idx.shape == (len(q), k)
+        assert np.array_equal(idx, np.argsort(d, axis=1, kind="stable")[:, :k])
+        assert (cnt == k).all()
+    launches = [b for b in eng.batches if b[0] == "knn"][1:]
+    # k = 5 and 7 (capacity class 8) ran as one k = 7 launch; k = 20 on its own
+    assert sorted(b[2] for b in launches) == [7, 20]
     srv.close()
