@@ -216,6 +216,17 @@ PPTKG_API int pptkg_multi_normals(const pptkg_tree* const* trees, int ntrees, co
  * V[i, j, :] = j-th eigenvector (estimate_normals.cpp:96-99). */
 PPTKG_API int pptkg_eigh3(const void* A, int64_t m, int dtype, int mem, void* w, void* V, int layout, void* stream);
 
+/* Covariances of neighbourhood lists (replaces the per-neighbourhood
+ * vfuncs chain MEAN / DOT(TRANSPOSE(Y), Y) that pptk's expression layer
+ * evaluates, pptk/points/expr.py:27-72, vfuncs/vfuncs.cpp `_mean`, `_dot`,
+ * `_transpose`): for neighbourhood i, the rows indices[offsets[i] ..
+ * offsets[i+1]) of the n x 3 points (F32/F64); out_cov (m x 3 x 3,
+ * row-major) = Y^T Y / count with Y the rows minus their mean.  Feed it to
+ * pptkg_eigh3 for the `_eigh` step.  An index outside [0, n) is
+ * PPTKG_E_RANGE. */
+PPTKG_API int pptkg_nbhd_covariance(const void* points, int64_t n, int dtype, int mem, const int64_t* offsets,
+                                   const int32_t* indices, int64_t m, void* out_cov, void* stream);
+
 /* Instrumentation (no reference counterpart).  Stage timing records CUDA
  * events on the launching stream around each stage ("build", "order",
  * "knn", "normals", "rnear_count", "rnear_fill", "h2d", "d2h");

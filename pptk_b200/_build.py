@@ -45,6 +45,15 @@ def _headers():
     return hs
 
 
+def _included_sources(src):
+    """.cu files that `src` includes (query_d2.cu / query_d4.cu include
+    query.cu to instantiate it for another dimension)."""
+    with open(src) as f:
+        text = f.read()
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+            if f.endswith(".cu") and f'#include "{f}"' in text]
+
+
 def _stale(target, deps):
     if not os.path.exists(target):
         return True
@@ -61,7 +70,7 @@ def build(force=False, verbose=False, extra_flags=()):
     jobs = []
     for s in srcs:
         o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
-        if force or _stale(o, [s] + hdrs + [__file__]):
+        if force or _stale(o, [s] + _included_sources(s) + hdrs + [__file__]):
             jobs.append((s, o))
 
     def compile_one(job):

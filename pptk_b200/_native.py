@@ -54,6 +54,7 @@ SIGNATURES = {
     "pptkg_estimate_normals": [_vp, _i64, _int, _int, _int, _flt, _vp, _i64, _int, _int, _vp, _vp, _vp, _vp],
     "pptkg_tree_normals": [_vp, _vp, _i64, _int, _int, _flt, _int, _int, _vp, _vp, _vp, _vp],
     "pptkg_eigh3": [_vp, _i64, _int, _int, _vp, _vp, _int, _vp],
+    "pptkg_nbhd_covariance": [_vp, _i64, _int, _int, _vp, _vp, _i64, _vp, _vp],
     "pptkg_forest_build": [_vp, _i64, _int, _int, _int, _vp, _int, _int, _dbl, _vp, _pvp],
     "pptkg_forest_info": [_vp, _pint, _vp],
     "pptkg_forest_ref_nodes": [_vp, _int, _vp, _i64, _pi64],

@@ -108,8 +108,21 @@ void dispatch_build(int dtype, int dim, F&& f) {
 
 template <typename F>
 void dispatch_query(const TreeBase* t, F&& f) {
-  if (t->dim != 3) throw Error(E_UNSUPPORTED, "queries on 2-d and 4-d trees are not implemented on the GPU yet");
+  if (t->dim != 3) throw Error(E_UNSUPPORTED, "forest and multi-tree queries need 3-d trees");
   dispatch_float(t->dtype, [&](auto tt) { f(tt, Dim<3>()); });
+}
+
+// kNN / r-near on single trees of any built dimension (2, 3, 4).
+template <typename F>
+void dispatch_query_dims(const TreeBase* t, F&& f) {
+  dispatch_float(t->dtype, [&](auto tt) {
+    switch (t->dim) {
+      case 2: f(tt, Dim<2>()); break;
+      case 3: f(tt, Dim<3>()); break;
+      case 4: f(tt, Dim<4>()); break;
+      default: throw Error(E_TYPE, "k-d tree dim must be 2, 3 or 4");
+    }
+  });
 }
 
 const TreeBase* tree_of(const pptkg_tree* t) {
@@ -489,7 +502,7 @@ int pptkg_knn(const pptkg_tree* tree, const void* queries, int64_t m, int qdtype
     if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
     if (qdtype != F32 && qdtype != F64) throw Error(E_TYPE, "query points must be float32 or float64");
     if (m && (!queries || !out_idx)) throw Error(E_INVALID, "null array");
-    dispatch_query(t, [&](auto tt, auto d) {
+    dispatch_query_dims(t, [&](auto tt, auto d) {
       typedef decltype(tt) T;
       constexpr int Dm = decltype(d)::value;
       const size_t qn = (size_t)m * Dm;
@@ -524,7 +537,7 @@ int pptkg_knn_self(const pptkg_tree* tree, const int32_t* indices, int64_t m, in
     if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
     if (!indices && m > t->n) throw Error(E_RANGE, "query rows exceed the point count");
     if (m && !out_idx) throw Error(E_INVALID, "out_idx is null");
-    dispatch_query(t, [&](auto tt, auto d) {
+    dispatch_query_dims(t, [&](auto tt, auto d) {
       typedef decltype(tt) T;
       constexpr int Dm = decltype(d)::value;
       Staged<int32_t> qi(indices, (size_t)m, mem, true, S(stream));
@@ -550,7 +563,7 @@ int pptkg_rnear_count(const pptkg_tree* tree, const void* queries, const int32_t
     if (m < 0 || m > INT32_MAX) throw Error(E_INVALID, "query count out of range");
     if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
     if (!out_offsets) throw Error(E_INVALID, "out_offsets is null");
-    dispatch_query(t, [&](auto tt, auto d) {
+    dispatch_query_dims(t, [&](auto tt, auto d) {
       typedef decltype(tt) T;
       constexpr int Dm = decltype(d)::value;
       RnearArgs a;
@@ -573,7 +586,7 @@ int pptkg_rnear_fill(const pptkg_tree* tree, const void* queries, const int32_t*
     if (m < 0 || m > INT32_MAX) throw Error(E_INVALID, "query count out of range");
     if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
     if (!offsets) throw Error(E_INVALID, "offsets is null");
-    dispatch_query(t, [&](auto tt, auto d) {
+    dispatch_query_dims(t, [&](auto tt, auto d) {
       typedef decltype(tt) T;
       constexpr int Dm = decltype(d)::value;
       RnearArgs a;
@@ -658,6 +671,35 @@ int pptkg_eigh3(const void* A, int64_t m, int dtype, int mem, void* w, void* V, 
       eigh3_batched<T>(a.d, m, ww.d, vv.d, layout, S(stream));
       ww.flush(S(stream));
       vv.flush(S(stream));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+  });
+}
+
+int pptkg_nbhd_covariance(const void* points, int64_t n, int dtype, int mem, const int64_t* offsets,
+                          const int32_t* indices, int64_t m, void* out_cov, void* stream) {
+  return guarded([&] {
+    if (n < 0 || m < 0) throw Error(E_INVALID, "negative count");
+    if (m && (!points || !offsets || !out_cov)) throw Error(E_INVALID, "null array");
+    dispatch_float(dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      int64_t total = 0;
+      if (m) {
+        if (mem == PPTKG_MEM_HOST) {
+          total = offsets[m];
+        } else {
+          PPTKG_CUDA(cudaMemcpyAsync(&total, offsets + m, sizeof(int64_t), cudaMemcpyDefault, S(stream)));
+          PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+        }
+      }
+      if (total < 0) throw Error(E_INVALID, "negative offsets");
+      if (total && !indices) throw Error(E_INVALID, "indices is null");
+      Staged<T> p(points, (size_t)n * 3, mem, true, S(stream));
+      Staged<int64_t> o(offsets, (size_t)m + 1, mem, true, S(stream));
+      Staged<int32_t> ix(indices, (size_t)total, mem, true, S(stream));
+      Staged<T> c(out_cov, (size_t)m * 9, mem, false, S(stream));
+      nbhd_covariance<T>(p.d, n, o.d, ix.d, total, m, c.d, S(stream));
+      c.flush(S(stream));
       PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
     });
   });

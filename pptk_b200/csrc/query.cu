@@ -228,7 +228,7 @@ __global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
   key[i] = min(max(k, 0), tv.nv);
 }
 
-__global__ void k_check_idx(const int* idx, int m, int n, int* status) {
+static __global__ void k_check_idx(const int* idx, int m, int n, int* status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m && (idx[i] < 0 || idx[i] >= n)) atomicExch(status, 4);
 }
@@ -248,7 +248,7 @@ static void check_indices(const TreeBase* t, const QuerySpec& qs, cudaStream_t s
 
 // Tree position of each index query (nv for dropped points and, when the
 // indices are unchecked, for indices outside [0, n)).
-__global__ void k_idxkey(const int* idx, const int* fwd, int m, int n, int nv, int* key) {
+static __global__ void k_idxkey(const int* idx, const int* fwd, int m, int n, int nv, int* key) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const int o = idx ? idx[i] : i;
@@ -266,12 +266,12 @@ static int order_shift(int nv, int m) {
   return s;
 }
 
-__global__ void k_hist(const int* key, int m, int shift, int* hist) {
+static __global__ void k_hist(const int* key, int m, int shift, int* hist) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) atomicAdd(&hist[key[i] >> shift], 1);
 }
 
-__global__ void k_place(const int* key, int m, int shift, int* cursor, int* order) {
+static __global__ void k_place(const int* key, int m, int shift, int* cursor, int* order) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) order[atomicAdd(&cursor[key[i] >> shift], 1)] = i;
 }
@@ -397,6 +397,14 @@ DistT radius2(double dmax) {
   return r * r;
 }
 
+static void check_status(int* d_status, cudaStream_t st, const char* what) {
+  int h = 0;
+  PPTKG_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (h == 4) throw Error(E_RANGE, std::string(what) + ": query index outside of its tree's [0, n)");
+  if (h) throw Error(E_DEVICE, std::string(what) + ": device traversal check failed (code " + std::to_string(h) + ")");
+}
+
 // The status word of one query call: the thread's status sink when one is
 // set (nothing is read back), else a fresh zeroed word checked at the end.
 struct StatusWord {
@@ -412,20 +420,11 @@ struct StatusWord {
     }
   }
   int* get() const { return p; }
-  void check(cudaStream_t st, const char* what);
+  void check(cudaStream_t st, const char* what) {
+    if (!g_status_sink) check_status(p, st, what);
+  }
 };
 
-static void check_status(int* d_status, cudaStream_t st, const char* what) {
-  int h = 0;
-  PPTKG_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PPTKG_CUDA(cudaStreamSynchronize(st));
-  if (h == 4) throw Error(E_RANGE, std::string(what) + ": query index outside of its tree's [0, n)");
-  if (h) throw Error(E_DEVICE, std::string(what) + ": device traversal check failed (code " + std::to_string(h) + ")");
-}
-
-void StatusWord::check(cudaStream_t st, const char* what) {
-  if (!g_status_sink) check_status(p, st, what);
-}
 
 template <typename T, int D>
 void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32_t* d_idx, int32_t* d_cnt,
@@ -962,7 +961,7 @@ void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStre
 }
 
 // ------------------------------------------------------------ forests ----
-__global__ void k_warp_cloud(const int64_t* slot_off, int ncloud, int64_t nwarps, int* warp_cloud) {
+static __global__ void k_warp_cloud(const int64_t* slot_off, int ncloud, int64_t nwarps, int* warp_cloud) {
   const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= nwarps) return;
   const int64_t s = w * 32;
@@ -1060,12 +1059,15 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
   status.check(st, "forest normals");
 }
 
+#ifndef PPTKG_QUERY_DIM
 template void forest_knn<float, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
 template void forest_knn<double, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
 template void forest_normals<float>(const TreeBase*, int, float, int, int, double, float*, float*, int32_t*,
                                     cudaStream_t);
 template void forest_normals<double>(const TreeBase*, int, float, int, int, double, double*, double*, int32_t*,
                                      cudaStream_t);
+#endif  // PPTKG_QUERY_DIM
+
 
 // ---------------------------------------------------- multi-tree batches --
 // Device tables of a multi-tree batch: TreeViews, per-warp group, slot and
@@ -1136,7 +1138,7 @@ static TreeBase* bounds_tree(int depth, int n_nodes) {
   return b;
 }
 
-__global__ void k_order_rows(const int* local, int m, int base, int* out) {
+static __global__ void k_order_rows(const int* local, int m, int base, int* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) out[i] = base + (local ? local[i] : i);
 }
@@ -1231,6 +1233,7 @@ void multi_normals(const TreeBase* const* trees, int ntrees, const int32_t* d_id
   check_status(status.get(), st, "multi-tree normals");
 }
 
+#ifndef PPTKG_QUERY_DIM
 template void multi_knn<float, 3>(const TreeBase* const*, int, const void*, int, const int64_t*, int, double, int32_t*,
                                   int32_t*, cudaStream_t);
 template void multi_knn<double, 3>(const TreeBase* const*, int, const void*, int, const int64_t*, int, double,
@@ -1239,7 +1242,10 @@ template void multi_normals<float>(const TreeBase* const*, int, const int32_t*, 
                                    double, float*, float*, int32_t*, cudaStream_t);
 template void multi_normals<double>(const TreeBase* const*, int, const int32_t*, const int64_t*, int, float, int, int,
                                     double, double*, double*, int32_t*, cudaStream_t);
+#endif  // PPTKG_QUERY_DIM
 
+
+#ifndef PPTKG_QUERY_DIM
 // ------------------------------------------- allocation-free normals ----
 // Scratch of pptkg_tree_normals_noalloc, resident on every GPU that loads the
 // library: [0] status word, [1] FP64 re-solve queue length, then (from int 64,
@@ -1335,6 +1341,8 @@ template void normals_noalloc<float>(const TreeBase*, const int32_t*, int64_t, i
 template void normals_noalloc<double>(const TreeBase*, const int32_t*, int64_t, int, float, int, int, double*,
                                       double*, int32_t*, cudaStream_t);
 
+#endif  // PPTKG_QUERY_DIM
+
 #define PPTKG_INST_Q(T, D)                                                                                 \
   template void knn_query<T, D>(const TreeBase*, const QuerySpec&, int, double, int32_t*, int32_t*,        \
                                 cudaStream_t);                                                             \
@@ -1342,6 +1350,11 @@ template void normals_noalloc<double>(const TreeBase*, const int32_t*, int64_t, 
   template void rnear_fill<T, D>(const TreeBase*, const QuerySpec&, double, const int64_t*, int32_t*,      \
                                  cudaStream_t);
 
+// This file builds the 3-d query paths and everything 3-d only (normals,
+// forests, multi-tree batches, the allocation-free entry point).
+// query_d2.cu / query_d4.cu include it with PPTKG_QUERY_DIM set and build
+// only the kNN and r-near paths of that dimension, in parallel.
+#ifndef PPTKG_QUERY_DIM
 PPTKG_INST_Q(float, 3)
 PPTKG_INST_Q(double, 3)
 
@@ -1351,5 +1364,9 @@ template void normals_query<double>(const TreeBase*, const QuerySpec&, int, floa
                                     int32_t*, cudaStream_t);
 template void eigh3_batched<float>(const float*, int64_t, float*, float*, int, cudaStream_t);
 template void eigh3_batched<double>(const double*, int64_t, double*, double*, int, cudaStream_t);
+#else
+PPTKG_INST_Q(float, PPTKG_QUERY_DIM)
+PPTKG_INST_Q(double, PPTKG_QUERY_DIM)
+#endif
 
 }  // namespace pptkg

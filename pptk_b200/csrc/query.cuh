@@ -70,4 +70,11 @@ void normals_noalloc(const TreeBase* t, const int32_t* d_idx, int64_t m, int k, 
 template <typename T>
 void eigh3_batched(const T* d_A, int64_t m, T* d_w, T* d_V, int layout, cudaStream_t st);
 
+
+// Centred covariances of m neighbourhoods given as CSR lists (offsets m+1,
+// `total` indices into the n x 3 points); C is m x 3 x 3 row-major (pca.cu).
+template <typename T>
+void nbhd_covariance(const T* d_pts, int64_t n, const int64_t* d_off, const int32_t* d_idx, int64_t total, int64_t m,
+                     T* d_C, cudaStream_t st);
+
 }  // namespace pptkg

@@ -37,3 +37,45 @@ def eigh3(A, layout="columns"):
     V = np.empty((m, 3, 3), a.dtype)
     N.call("pptkg_eigh3", N.ptr(a), m, _CODES[a.dtype], N.MEM_HOST, N.ptr(w), N.ptr(V), lay, None)
     return w, V
+
+
+def _csr(nbhds):
+    """(offsets int64 m+1, indices int32) from a list of index arrays (the
+    _query / Points.nbhds form), a (offsets, indices) pair, or a dense
+    (indices m x k, counts m) pair from kdtree.knn."""
+    if isinstance(nbhds, tuple) and len(nbhds) == 2:
+        a, b = (np.asarray(x.cpu() if hasattr(x, "cpu") else x) for x in nbhds)
+        if a.ndim == 2:  # dense kNN result: (indices m x k, counts m)
+            cnt = b.astype(np.int64)
+            off = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+            keep = np.arange(a.shape[1])[None, :] < cnt[:, None]
+            return off, np.ascontiguousarray(a[keep], dtype=np.int32)
+        return np.ascontiguousarray(a, dtype=np.int64), np.ascontiguousarray(b, dtype=np.int32)
+    rows = [np.asarray(r, dtype=np.int64).reshape(-1) for r in nbhds]
+    off = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int64)
+    idx = np.concatenate(rows).astype(np.int32) if rows else np.zeros(0, np.int32)
+    return off, np.ascontiguousarray(idx)
+
+
+def nbhd_covariance(points, nbhds):
+    """Covariance Y^T Y / count of every neighbourhood (Y its points minus
+    their mean): what pptk's expression layer builds per neighbourhood with
+    MEAN / DOT / TRANSPOSE (pptk/points/expr.py:27-72).  points: n x 3
+    float32/float64 numpy array; nbhds as for `nbhd_pca`.  Returns m x 3 x 3."""
+    P = np.ascontiguousarray(np.asarray(points))
+    if P.dtype not in _CODES or P.ndim != 2 or P.shape[1] != 3:
+        raise TypeError("points must be an n x 3 float32 or float64 array")
+    off, idx = _csr(nbhds)
+    m = len(off) - 1
+    C = np.empty((m, 3, 3), P.dtype)
+    N.call("pptkg_nbhd_covariance", N.ptr(P), P.shape[0], _CODES[P.dtype], N.MEM_HOST, N.ptr(off), N.ptr(idx), m,
+           N.ptr(C), None, where="nbhd_covariance()")
+    return C
+
+
+def nbhd_pca(points, nbhds):
+    """PCA of every neighbourhood on the GPU: (w (m, 3) ascending, V (m, 3, 3)
+    with V[i][:, j] the j-th eigenvector -- vfuncs `_eigh`'s layout).  nbhds:
+    a list of index arrays (as returned by kdtree._query / Points.nbhds), an
+    (offsets, indices) CSR pair, or kdtree.knn's (indices, counts)."""
+    return eigh3(nbhd_covariance(points, nbhds), layout="columns")

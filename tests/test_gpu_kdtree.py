@@ -226,3 +226,33 @@ def test_scene_properties_at_scale(gpu, port):
     off, out = gpu.kdtree.rnear(t, sample, 0.5)
     ooff, oout = o.rnear_self(sample, 0.5)
     assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+
+
+@pytest.mark.parametrize("dim", [2, 4])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_2d_and_4d_trees_match_oracle(gpu, port, dim, dtype):
+    rng = np.random.default_rng(10 + dim)
+    P = rng.random((40_000, dim)).astype(dtype)
+    P[::997] = P[1::997]  # a few duplicate points (distance ties)
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    assert np.array_equal(t.reverse_indices(), o.reverse_indices())
+    gi, gc = gpu.kdtree.knn(t, None, 9)
+    oi, oc = o.knn_self(np.arange(len(P), dtype=np.int32), 9)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    q = rng.random((3000, dim)).astype(dtype)
+    gi, gc = gpu.kdtree.knn(t, q, 9, dmax=0.05)
+    oi, oc = o.knn(q, 9, dmax=float(np.float32(0.05)))
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    r = 0.03 if dim == 2 else 0.12
+    off, out = gpu.kdtree.rnear(t, q, r)
+    ooff, oout = o.rnear(q, float(np.float32(r)))
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+    sidx = np.arange(0, len(P), 13, dtype=np.int32)
+    off, out = gpu.kdtree.rnear(t, sidx, r)
+    ooff, oout = o.rnear_self(sidx, float(np.float32(r)))
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+    # the list form of _query
+    rows = gpu.kdtree._query(t, q[:50], k=4)
+    ei, _ = o.knn(q[:50], 4)
+    assert all(np.array_equal(a, b) for a, b in zip(rows, ei))

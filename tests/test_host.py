@@ -117,3 +117,19 @@ def test_synthetic_workloads_are_seeded():
     assert p.dtype == np.float64 and (p[:, 0] > 9e4).all()
     s = synth.ragged_sizes(64)
     assert (s >= 1000).all() and (s <= 200_000).all()
+
+
+def test_points_track_writes_through_views():
+    from pptk_b200.points import Points, points
+    P = points(np.zeros((10, 3), np.float32))
+    assert not P.flags.writeable
+    with pytest.raises(ValueError):
+        np.ndarray.__setitem__(P, 0, 1.0)  # plain writes are refused
+    t0 = Points._last_modified[P._memloc]
+    v = P[2:5]
+    assert v._memloc == P._memloc  # a view shares the buffer's record
+    v += 1
+    assert Points._last_modified[P._memloc] >= t0 and P[2, 0] == 1.0
+    c = P.copy()
+    assert c._memloc != P._memloc and not c.flags.writeable
+    assert len(P.NBHDS(queries=[1, 2, 3], k=2)) == 3
