@@ -276,7 +276,15 @@ def device_timed(ctx, fn, steps):
     return e0.elapsed_time(e1) / steps, int(launches), clocks.stop()
 
 
-def roofline(ctx, stage_name, queries):
+# DRAM bytes per query of k_normals (k=16, float32) measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's queries):
+# tree-order queries (profiles/k_normals_plain_lidar8M.md) and scattered
+# serving queries (profiles/k_normals_k_knn_serving_lidar8M.md); the bench's
+# per-launch traffic is this figure times the queries of a launch.
+TRAFFIC_PER_QUERY = {"tree_order": 111.8, "scattered": 160.5}
+
+
+def roofline(ctx, stage_name, queries, traffic_kind):
     peak, peak_kind = load_peaks()
     t_ms, cnt = ctx.stage(stage_name)
     if not cnt or t_ms <= 0:
@@ -284,9 +292,13 @@ def roofline(ctx, stage_name, queries):
     per_launch_ms = t_ms / cnt
     bytes_per_launch = BYTES_PER_QUERY * queries / cnt
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+    traffic = TRAFFIC_PER_QUERY[traffic_kind] * queries / cnt
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "k_normals (fused kNN+PCA)", "peak_kind": f"{peak_kind} hbm_gbs",
-            "launches": cnt, "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch}
+            "traffic": traffic, "kernel": "k_normals (fused kNN+PCA)", "peak_kind": f"{peak_kind} hbm_gbs",
+            "launches": cnt, "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch,
+            "traffic_source": f"ncu DRAM bytes per query ({traffic_kind} queries, 8M-point capture) x queries "
+                              "per launch",
+            "limiter": "instruction issue (ALU pipe ~70 % busy, DRAM < 1.1 % of peak in the ncu captures)"}
 
 
 BUILD_STAGES = ("build", "build.prep", "build.attempt", "build.levels", "build.subtree", "build.finish",
@@ -314,7 +326,7 @@ def run_plain_workload(args, ctx):
     for nm in BUILD_STAGES:
         t_, c_ = ctx.stage(nm)
         stages[nm] = t_ / max(c_, 1) if c_ else 0.0
-    roof = roofline(ctx, "normals", n * args.steps)
+    roof = roofline(ctx, "normals", n * args.steps, "tree_order")
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
     value = ctx.throughput(n, ms / 1e3)
@@ -373,7 +385,7 @@ def run_ragged_workload(args, ctx):
     for nm in ("build", "build.levels", "build.subtree", "forest.knn", "forest.normals"):
         t_, c_ = ctx.stage(nm)
         stages[nm] = t_ / max(c_, 1) if c_ else 0.0
-    roof = roofline(ctx, "forest.normals", n * args.steps)
+    roof = roofline(ctx, "forest.normals", n * args.steps, "tree_order")
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
     value = ctx.throughput(n, ms / 1e3)
@@ -608,7 +620,7 @@ def run_serving_workload(args, ctx):
     for nm in ("multi.knn", "multi.normals", "normals.refine64", "order"):
         t_, c_ = ctx.stage(nm)
         stages[nm] = {"ms_total_per_step": t_ / args.steps, "launches_per_step": c_ / args.steps}
-    roof = roofline(ctx, "multi.normals", n_norm * args.steps)
+    roof = roofline(ctx, "multi.normals", n_norm * args.steps, "scattered")
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
     value = ctx.throughput(per_step, ms / 1e3)
