@@ -73,7 +73,11 @@ PPTKG_API int pptkg_last_error(char* buf, size_t len);
  * (pptk/kdtree/kdtree_wrapper.cpp:76-104, :281-304) and the KdTree
  * constructor (pptk/kdtree/src/kdtree-impl.h:773-833).  Rows holding a NaN or
  * inf coordinate are left out, as in the reference.  The tree owns a copy of
- * the points.  dtype: PPTKG_F32 or PPTKG_F64; dim: 2, 3 or 4. */
+ * the points.  dtype: any PPTKG_* point type (float32, float64, int8 ...
+ * uint64); dim: 2, 3 or 4.  Integer trees are built in their own type, as
+ * the reference builds them, and answer queries in float, the reference's
+ * distance type for integers (accumulator.h:16-19); pptkg_tree_info reports
+ * the input type. */
 PPTKG_API int pptkg_tree_build(const void* points, int64_t n, int dim, int dtype, int mem, int max_leaf_size,
                      double empty_split, void* stream, pptkg_tree** out);
 

@@ -106,6 +106,38 @@ void dispatch_build(int dtype, int dim, F&& f) {
   });
 }
 
+// Every point type the reference builds trees of (kdtree_wrapper.cpp:15-55).
+template <typename F>
+void dispatch_any(int dtype, F&& f) {
+  switch (dtype) {
+    case F32: f(float()); break;
+    case F64: f(double()); break;
+    case I8: f(int8_t()); break;
+    case I16: f(int16_t()); break;
+    case I32: f(int32_t()); break;
+    case I64: f(int64_t()); break;
+    case U8: f(uint8_t()); break;
+    case U16: f(uint16_t()); break;
+    case U32: f(uint32_t()); break;
+    case U64: f(uint64_t()); break;
+    default: throw Error(E_TYPE, "unsupported point dtype code " + std::to_string(dtype));
+  }
+}
+
+template <typename F>
+void dispatch_build_any(int dtype, int dim, F&& f) {
+  dispatch_any(dtype, [&](auto t) {
+    if (dim == 2)
+      f(t, Dim<2>());
+    else if (dim == 3)
+      f(t, Dim<3>());
+    else if (dim == 4)
+      f(t, Dim<4>());
+    else
+      throw Error(E_TYPE, "k-d tree dim must be 2, 3 or 4 (got " + std::to_string(dim) + ")");
+  });
+}
+
 template <typename F>
 void dispatch_query(const TreeBase* t, F&& f) {
   if (t->dim != 3) throw Error(E_UNSUPPORTED, "forest and multi-tree queries need 3-d trees");
@@ -206,6 +238,7 @@ static void stage_rnear(RnearArgs& a, const pptkg::TreeBase* t, const void* quer
 static void run_normals(const TreeBase* t, const int32_t* indices, int64_t m, int mem, int k, float r, int num_eigen,
                         int precision, void* out_evecs, void* out_evals, int32_t* out_sizes, cudaStream_t st) {
   if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+  if (t->rec_dtype != F32 && t->rec_dtype != F64) throw Error(E_TYPE, "normals need float32 or float64 points");
   if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
   if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
   if (k == 0) throw Error(E_INVALID, "k cannot be zero");
@@ -254,7 +287,7 @@ int pptkg_tree_build(const void* points, int64_t n, int dim, int dtype, int mem,
     if (n < 0) throw Error(E_INVALID, "negative point count");
     if (n > 0 && !points) throw Error(E_INVALID, "points is null");
     if (!(empty_split >= 0.0)) throw Error(E_INVALID, "emptysplit must be non-negative");
-    dispatch_build(dtype, dim, [&](auto t, auto d) {
+    dispatch_build_any(dtype, dim, [&](auto t, auto d) {
       typedef decltype(t) T;
       constexpr int Dm = decltype(d)::value;
       Staged<T> in(points, (size_t)n * Dm, mem, true, S(stream));
@@ -394,6 +427,8 @@ int pptkg_multi_normals(const pptkg_tree* const* trees, int ntrees, const int32_
     if (!row_offsets || row_offsets[0] != 0) throw Error(E_INVALID, "row offsets must start at 0");
     const int64_t m = row_offsets[ntrees];
     if (v[0]->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+    for (const TreeBase* x : v)
+      if (x->rec_dtype != F32 && x->rec_dtype != F64) throw Error(E_TYPE, "normals need float32 or float64 points");
     if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
     if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
     if (m && !indices) throw Error(E_INVALID, "indices is null");
@@ -424,7 +459,7 @@ int pptkg_tree_info(const pptkg_tree* tree, int64_t* n, int64_t* n_valid, int* d
     if (n) *n = t->n;
     if (n_valid) *n_valid = t->nv;
     if (dim) *dim = t->dim;
-    if (dtype) *dtype = t->dtype;
+    if (dtype) *dtype = t->rec_dtype;
     if (n_records) *n_records = t->n_recs;
     if (depth) *depth = t->depth;
   });
@@ -455,7 +490,7 @@ static int ref_nodes(const pptkg_tree* tree, int cloud, double* out, int64_t cap
     const TreeBase* t = tree_of(tree);
     if (cloud < -1 || cloud >= t->ncloud) throw Error(E_INVALID, "cloud index out of range");
     DeviceGuard g(t->device);
-    dispatch_build(t->dtype, t->dim, [&](auto tt, auto d) {
+    dispatch_build_any(t->rec_dtype, t->dim, [&](auto tt, auto d) {
       typedef decltype(tt) T;
       constexpr int Dm = decltype(d)::value;
       std::vector<Rec<T, Dm>> recs(t->n_recs);
@@ -486,7 +521,7 @@ int pptkg_tree_set_bucket(pptkg_tree* tree, int bucket, void* stream) {
     TreeBase* t = tree->t.get();
     DeviceGuard g(t->device);
     if (bucket < 1 || bucket > 4096) throw Error(E_INVALID, "bucket must be in [1, 4096]");
-    dispatch_build(t->dtype, t->dim, [&](auto tt, auto d) {
+    dispatch_build_any(t->rec_dtype, t->dim, [&](auto tt, auto d) {
       make_tnodes<decltype(tt), decltype(d)::value>(t, bucket, S(stream));
     });
   });
@@ -645,6 +680,7 @@ int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* indices, i
     const TreeBase* t = tree_of(tree);
     DeviceGuard g(t->device);
     if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+    if (t->rec_dtype != F32 && t->rec_dtype != F64) throw Error(E_TYPE, "normals need float32 or float64 points");
     if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
     if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
     if (precision < PPTKG_PREC_AUTO || precision > PPTKG_PREC_FP64) throw Error(E_INVALID, "unknown precision");

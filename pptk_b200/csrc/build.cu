@@ -59,9 +59,33 @@ struct BuildCtl {
 // ----------------------------------------------------------------- helpers
 template <typename T>
 __device__ __forceinline__ T midpoint_ref(T a, T b) {
-  // kdtree-impl.h:167-173 (signed / floating form)
-  if ((a >= (T)0 && b >= (T)0) || (a < (T)0 && b < (T)0)) return xadd(xdiv(xsub(b, a), (T)2), a);
-  return xdiv(xadd(a, b), (T)2);
+  if constexpr (std::is_unsigned<T>::value) {
+    // kdtree-impl.h:161-164 (unsigned form), in C++ integer promotion
+    if (a < b) {
+      const T t = a;
+      a = b;
+      b = t;
+    }
+    return (T)((a - b) / 2 + b);
+  } else if constexpr (std::is_integral<T>::value) {
+    // kdtree-impl.h:167-173 (signed form), in C++ integer promotion
+    if ((a >= 0 && b >= 0) || (a < 0 && b < 0)) return (T)((b - a) / (T)2 + a);
+    return (T)((a + b) / (T)2);
+  } else {
+    // the same signed form in floating point, one rounding per operation
+    if ((a >= (T)0 && b >= (T)0) || (a < (T)0 && b < (T)0)) return xadd(xdiv(xsub(b, a), (T)2), a);
+    return xdiv(xadd(a, b), (T)2);
+  }
+}
+
+// `T width = max - min` of ComputeSplit (kdtree-impl.h:179): integer types
+// wrap as the reference's conversion back to T does.
+template <typename T>
+__device__ __forceinline__ T width_ref(T lo, T hi) {
+  if constexpr (std::is_integral<T>::value)
+    return (T)(hi - lo);
+  else
+    return xsub(hi, lo);
 }
 
 __device__ __forceinline__ double max0(double x) { return (0.0 < x) ? x : 0.0; }
@@ -117,7 +141,7 @@ __device__ void node_logic(int size, long long n_orig, bool is_top, T lo[D], T h
     sd = 0;
     sv = (T)0;
     for (int i = 0; i < D; i++) {
-      T w = xsub(thi[i], tlo[i]);
+      T w = width_ref(tlo[i], thi[i]);
       if (w >= maxw) {
         maxw = w;
         sd = i;
@@ -150,7 +174,7 @@ __global__ void k_valid(const T* __restrict__ in, int64_t n, int* __restrict__ f
   if (i >= n) return;
   bool ok = true;
 #pragma unroll
-  for (int d = 0; d < D; d++) ok = ok && isfinite(in[i * D + d]);
+  for (int d = 0; d < D; d++) ok = ok && valid_coord(in[i * D + d]);
   flag[i] = ok ? 1 : 0;
 }
 
@@ -167,7 +191,7 @@ __global__ void k_compact(const T* __restrict__ in, int64_t n, const int* __rest
 
 // valid_off[c] = number of valid rows before cloud c (the stable compaction
 // keeps every cloud's valid rows together, in order).
-__global__ void k_cloud_off(const int* off, const int64_t* orig_off, int ncloud, int64_t* valid_off) {
+static __global__ void k_cloud_off(const int* off, const int64_t* orig_off, int ncloud, int64_t* valid_off) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c <= ncloud) valid_off[c] = off[orig_off[c]];
 }
@@ -252,8 +276,8 @@ __global__ void k_seg_init(Seg<T, D>* segs, int lvl, const BuildCtl* ctl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ctl->level_cnt[lvl]) return;
   for (int d = 0; d < D; d++) {
-    segs[i].tlo[d] = ord_of(Limits<T>::max());
-    segs[i].thi[d] = ord_of(Limits<T>::lowest());
+    segs[i].tlo[d] = ord_t<T>(Limits<T>::max());
+    segs[i].thi[d] = ord_t<T>(Limits<T>::lowest());
   }
   segs[i].L1 = segs[i].L2 = 0;
   segs[i].act = 0;
@@ -310,8 +334,8 @@ __global__ void __launch_bounds__(BT) k_bbox(Seg<T, D>* segs, const int* tile_se
       a = min(a, shmn[d][w]);
       b = max(b, shmx[d][w]);
     }
-    atomicMin(&segs[s].tlo[d], ord_of(a));
-    atomicMax(&segs[s].thi[d], ord_of(b));
+    atomicMin(&segs[s].tlo[d], ord_t<T>(a));
+    atomicMax(&segs[s].thi[d], ord_t<T>(b));
   }
 }
 
@@ -323,8 +347,8 @@ __global__ void k_node(Seg<T, D>* segs, int lvl, BuildCtl* ctl, Rec<T, D>* recs,
   Seg<T, D>& g = segs[i];
   T tlo[D], thi[D], lo[D], hi[D];
   for (int d = 0; d < D; d++) {
-    tlo[d] = from_ord(g.tlo[d]);
-    thi[d] = from_ord(g.thi[d]);
+    tlo[d] = from_ord_t<T>(g.tlo[d]);
+    thi[d] = from_ord_t<T>(g.thi[d]);
     lo[d] = g.lo[d];
     hi[d] = g.hi[d];
   }
@@ -865,6 +889,69 @@ int small_capacity(int max_leaf, int& cap_list, size_t& smem) {
   return cap;
 }
 
+// ------------------------------------------------ integer point types ----
+// The reference computes every distance of an integer tree in float
+// (Accumulator, accumulator.h:16-19): each coordinate and box bound is
+// converted to float where it is read (kdtree-impl.h:331-339, box.h:157-198).
+// After the build (done exactly in T), the tree-ordered points and the
+// traversal boxes are stored as those float values, so the float query
+// kernels answer integer trees; the records stay in T.
+template <typename T, int D>
+__global__ void k_lower_points(const PointRec<T, D>* in, int64_t nv, PointRec<float, D>* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  PointRec<float, D> r;
+#pragma unroll
+  for (int d = 0; d < D; d++) r.c[d] = (float)in[i].c[d];
+  r.id = in[i].id;
+  out[i] = r;
+}
+
+template <typename T, int D>
+__global__ void k_lower_tnodes(const TNode<T, D>* in, int n, TNode<float, D>* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  TNode<float, D> t;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      t.lo[k][d] = (float)in[i].lo[k][d];
+      t.hi[k][d] = (float)in[i].hi[k][d];
+    }
+    t.ref[k] = in[i].ref[k];
+    t.cnt[k] = in[i].cnt[k];
+  }
+  out[i] = t;
+}
+
+template <typename T, int D>
+void lower_points(TreeBase* tree, cudaStream_t st) {
+  PointRec<float, D>* out = nullptr;
+  PPTKG_CUDA(cudaMallocAsync((void**)&out, std::max<int64_t>(tree->nv, 1) * sizeof(PointRec<float, D>), st));
+  if (tree->nv > 0) {
+    k_lower_points<T, D><<<(unsigned)((tree->nv + 255) / 256), 256, 0, st>>>((const PointRec<T, D>*)tree->pts,
+                                                                             tree->nv, out);
+    PPTKG_CHECK_LAUNCH();
+  }
+  PPTKG_CUDA(cudaFreeAsync(tree->pts, st));
+  tree->pts = out;
+  tree->dtype = F32;
+}
+
+template <typename T, int D>
+void lower_tnodes(TreeBase* tree, cudaStream_t st) {
+  TNode<float, D>* out = nullptr;
+  const int n = tree->n_tnodes;
+  PPTKG_CUDA(cudaMallocAsync((void**)&out, std::max(n, 1) * sizeof(TNode<float, D>), st));
+  if (n > 0) {
+    k_lower_tnodes<T, D><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const TNode<T, D>*)tree->tnodes, n, out);
+    PPTKG_CHECK_LAUNCH();
+  }
+  PPTKG_CUDA(cudaFreeAsync(tree->tnodes, st));
+  tree->tnodes = out;
+}
+
 template <typename T, int D>
 TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int ncloud, int max_leaf, double thr,
                        int bucket, cudaStream_t st) {
@@ -875,7 +962,8 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   keep_pool_cached(st);
   std::unique_ptr<TreeBase> tree(new TreeBase());
   tree->stream = st;
-  tree->dtype = sizeof(T) == 4 ? F32 : F64;
+  tree->dtype = std::is_same<T, double>::value ? F64 : F32;
+  tree->rec_dtype = dtype_code<T>();
   tree->dim = D;
   tree->n = n;
   tree->max_leaf = max_leaf;
@@ -1063,6 +1151,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
       tree->root_hi[d] = (double)r0.hi[d];
     }
   }
+  if constexpr (std::is_integral<T>::value) lower_points<T, D>(tree.get(), st);
   return tree.release();
 }
 
@@ -1107,9 +1196,11 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
   PPTKG_CUDA(cudaMemcpyAsync(tree->root_tnode_h.data(), tree->root_tnode, sizeof(int) * tree->ncloud,
                              cudaMemcpyDeviceToHost, st));
   tree->tdepth = tree->depth + 2;
+  if constexpr (std::is_integral<T>::value) lower_tnodes<T, D>(tree, st);
   PPTKG_CUDA(cudaStreamSynchronize(st));
 }
 
+#ifndef PPTKG_BUILD_INT
 size_t TreeBase::device_bytes() const {
   size_t ps = (dtype == F64 ? 8 : 4) * dim + 4;
   ps = (ps + 15) / 16 * 16;
@@ -1130,16 +1221,32 @@ TreeBase::~TreeBase() {
   if (warp_cloud) cudaFreeAsync(warp_cloud, stream);
 }
 
+#endif  // PPTKG_BUILD_INT
+
 #define PPTKG_INST_BUILD(T, D)                                                                                  \
   template TreeBase* build_tree<T, D>(const T*, int64_t, int, double, int, cudaStream_t);                      \
   template TreeBase* build_forest<T, D>(const T*, int64_t, const int64_t*, int, int, double, int, cudaStream_t); \
   template void make_tnodes<T, D>(TreeBase*, int, cudaStream_t);
 
+// This file builds float32 / float64 trees; build_int.cu includes it with
+// PPTKG_BUILD_INT set and builds the eight integer point types.
+#ifndef PPTKG_BUILD_INT
 PPTKG_INST_BUILD(float, 3)
 PPTKG_INST_BUILD(double, 3)
 PPTKG_INST_BUILD(float, 2)
 PPTKG_INST_BUILD(double, 2)
 PPTKG_INST_BUILD(float, 4)
 PPTKG_INST_BUILD(double, 4)
+#else
+#define PPTKG_INST_BUILD_DIMS(T) PPTKG_INST_BUILD(T, 2) PPTKG_INST_BUILD(T, 3) PPTKG_INST_BUILD(T, 4)
+PPTKG_INST_BUILD_DIMS(int8_t)
+PPTKG_INST_BUILD_DIMS(int16_t)
+PPTKG_INST_BUILD_DIMS(int32_t)
+PPTKG_INST_BUILD_DIMS(int64_t)
+PPTKG_INST_BUILD_DIMS(uint8_t)
+PPTKG_INST_BUILD_DIMS(uint16_t)
+PPTKG_INST_BUILD_DIMS(uint32_t)
+PPTKG_INST_BUILD_DIMS(uint64_t)
+#endif
 
 }  // namespace pptkg

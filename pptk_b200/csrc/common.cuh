@@ -3,6 +3,9 @@
 // floating point values for atomic min/max, and error plumbing.
 #pragma once
 
+#include <limits>
+#include <type_traits>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -61,6 +64,14 @@ extern thread_local int* g_status_sink;
 // Identical to include/pptkg.h.
 enum DType { F32 = 0, F64 = 1, I8 = 2, I16 = 3, I32 = 4, I64 = 5, U8 = 6, U16 = 7, U32 = 8, U64 = 9 };
 
+template <typename T>
+constexpr int dtype_code() {
+  if constexpr (std::is_same<T, float>::value) return F32;
+  else if constexpr (std::is_same<T, double>::value) return F64;
+  else if constexpr (std::is_signed<T>::value) return sizeof(T) == 1 ? I8 : sizeof(T) == 2 ? I16 : sizeof(T) == 4 ? I32 : I64;
+  else return sizeof(T) == 1 ? U8 : sizeof(T) == 2 ? U16 : sizeof(T) == 4 ? U32 : U64;
+}
+
 inline int dtype_size(int dt) {
   switch (dt) {
     case F32: case I32: case U32: return 4;
@@ -76,14 +87,10 @@ inline int dtype_size(int dt) {
 template <typename T> struct DistOf { typedef float type; };
 template <> struct DistOf<double> { typedef double type; };
 
-template <typename T> struct Limits;
-template <> struct Limits<float> {
-  __host__ __device__ static float max() { return FLT_MAX; }
-  __host__ __device__ static float lowest() { return -FLT_MAX; }
-};
-template <> struct Limits<double> {
-  __host__ __device__ static double max() { return DBL_MAX; }
-  __host__ __device__ static double lowest() { return -DBL_MAX; }
+// Largest and lowest finite values of a point type (all ten pptk dtypes).
+template <typename T> struct Limits {
+  __host__ __device__ static constexpr T max() { return std::numeric_limits<T>::max(); }
+  __host__ __device__ static constexpr T lowest() { return std::numeric_limits<T>::lowest(); }
 };
 
 // --------------------------------------------- exact (uncontracted) math --
@@ -118,9 +125,48 @@ __host__ __device__ __forceinline__ double from_ord(unsigned long long u) {
   return *reinterpret_cast<double*>(&u);
 }
 
-template <typename T> struct OrdOf;
-template <> struct OrdOf<float> { typedef uint32_t type; };
-template <> struct OrdOf<double> { typedef unsigned long long type; };
+// The same monotone images for every point type (ord_t / from_ord_t):
+// floats as above; integers of up to 32 bits as unsigned 32-bit with the
+// sign bit flipped for signed types; 64-bit integers likewise in 64 bits.
+template <typename T> struct OrdOf {
+  typedef typename std::conditional<(sizeof(T) > 4), unsigned long long, uint32_t>::type type;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ typename OrdOf<T>::type ord_t(T v) {
+  typedef typename OrdOf<T>::type U;
+  if constexpr (std::is_floating_point<T>::value) {
+    return ord_of(v);
+  } else if constexpr (std::is_signed<T>::value) {
+    typedef typename std::conditional<(sizeof(T) > 4), long long, int32_t>::type S;
+    return (U)(S)v ^ ((U)1 << (sizeof(U) * 8 - 1));
+  } else {
+    return (U)v;
+  }
+}
+
+template <typename T>
+__host__ __device__ __forceinline__ T from_ord_t(typename OrdOf<T>::type u) {
+  typedef typename OrdOf<T>::type U;
+  if constexpr (std::is_floating_point<T>::value) {
+    return from_ord(u);
+  } else if constexpr (std::is_signed<T>::value) {
+    typedef typename std::conditional<(sizeof(T) > 4), long long, int32_t>::type S;
+    return (T)(S)(u ^ ((U)1 << (sizeof(U) * 8 - 1)));
+  } else {
+    return (T)u;
+  }
+}
+
+// A coordinate the reference keeps (ValidPointIndices drops NaN/inf rows;
+// integer coordinates are always kept).
+template <typename T>
+__host__ __device__ __forceinline__ bool valid_coord(T v) {
+  if constexpr (std::is_floating_point<T>::value)
+    return isfinite(v);
+  else
+    return true;
+}
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 __host__ __device__ __forceinline__ int div_up_dev(int a, int b) { return (a + b - 1) / b; }

@@ -71,7 +71,11 @@ struct TreeView {
 // concatenated array; cloud c's points occupy positions
 // [valid_off[c], valid_off[c+1]) and its traversals start at root_tnode[c].
 struct TreeBase {
-  int dtype = F32, dim = 3;
+  // dtype: type of the traversal data (points, TNodes), F32 or F64.
+  // rec_dtype: the input point type, in which the tree was built and its
+  // records are kept; an integer tree's traversal data is stored as the
+  // float values the reference's distance type (float) gives its coordinates.
+  int dtype = F32, dim = 3, rec_dtype = F32;
   int64_t n = 0, nv = 0;
   int n_recs = 0, n_tnodes = 0, depth = 0, tdepth = 0, bucket = 32;
   int max_leaf = 10;

@@ -81,7 +81,10 @@ def _build(data, numprocs=-1, maxleafsize=10, emptysplit=0.2):
 
     Parameters
     ----------
-    data : n x k numpy array (or CUDA torch tensor), float32 or float64, k in [2, 4].
+    data : n x k numpy array (or CUDA torch tensor) of float32, float64 or an
+        integer type (int8 ... uint64), k in [2, 4].  Integer trees are
+        built in their own type and answer queries in float32, the
+        reference's distance type for integers.
     numprocs : int, optional
         Accepted for compatibility; the build runs on the GPU.
     maxleafsize : int, optional
@@ -104,18 +107,18 @@ def _build(data, numprocs=-1, maxleafsize=10, emptysplit=0.2):
         raise RuntimeError(f"PerformAction(): Invalid k-d tree dim = {dim}.")
     if N.is_torch_cuda(a):
         import torch
-        if a.dtype not in (torch.float32, torch.float64):
-            raise NotImplementedError(f"k-d tree points of dtype {a.dtype} are not supported on the GPU path")
+        tcodes = {torch.float32: 0, torch.float64: 1, torch.int8: 2, torch.int16: 3, torch.int32: 4,
+                  torch.int64: 5, torch.uint8: 6}
+        if a.dtype not in tcodes:
+            raise RuntimeError(f"PerformAction_(): Invalid k-d tree type_num (dtype {a.dtype}).")
         a = a.contiguous()
-        code = 0 if a.dtype == torch.float32 else 1
+        code = tcodes[a.dtype]
         mem, stream, device = N.MEM_DEVICE, N.torch_stream(a.device), a.device
     else:
-        if a.dtype not in _FLOAT_CODES:
-            if a.dtype in N.DTYPE_CODES:
-                raise NotImplementedError(f"k-d tree points of dtype {a.dtype} are not supported on the GPU path")
+        if a.dtype not in N.DTYPE_CODES:
             raise RuntimeError(f"PerformAction_(): Invalid k-d tree type_num (dtype {a.dtype}).")
         a = np.ascontiguousarray(a)
-        code = _FLOAT_CODES[a.dtype]
+        code = N.DTYPE_CODES[a.dtype]
         mem, stream, device = N.MEM_HOST, None, None
     h = ctypes.c_void_p()
     N.call("pptkg_tree_build", N.ptr(a), int(m), int(dim), code, mem, maxleafsize, emptysplit, stream,
@@ -174,7 +177,7 @@ class _Batch:
                                      f"(expecting dim = {tree.dim}).")
                 q = queries
                 if q.dtype not in (torch.float32, torch.float64):
-                    q = q.to(torch.float64)
+                    q = q.to(torch.float32 if tree.dtype.kind in "iu" else torch.float64)
                 self.points = q.contiguous()
                 self.qdtype = 0 if q.dtype == torch.float32 else 1
                 self.m = int(q.shape[0])
@@ -189,7 +192,10 @@ class _Batch:
                                  f"(expecting dim = {tree.dim}).")
             q = queries
             if q.dtype not in _FLOAT_CODES:
-                q = q.astype(np.float64)
+                # integer trees compute in float32 (one conversion per
+                # coordinate, as the reference's (DistT)q); float trees
+                # take other query types through float64
+                q = q.astype(np.float32 if tree.dtype.kind in "iu" else np.float64)
             self.points = np.ascontiguousarray(q)
             self.qdtype = _FLOAT_CODES[self.points.dtype]
             self.m = self.points.shape[0]

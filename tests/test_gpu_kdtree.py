@@ -256,3 +256,50 @@ def test_2d_and_4d_trees_match_oracle(gpu, port, dim, dtype):
     rows = gpu.kdtree._query(t, q[:50], k=4)
     ei, _ = o.knn(q[:50], 4)
     assert all(np.array_equal(a, b) for a, b in zip(rows, ei))
+
+
+INT_TYPES = [np.int8, np.uint8, np.int16, np.uint16, np.int32, np.uint32, np.int64, np.uint64]
+
+
+@pytest.mark.parametrize("dtype", INT_TYPES)
+@pytest.mark.parametrize("dim", [2, 3])
+def test_integer_trees_match_oracle(gpu, port, dtype, dim):
+    # integer trees: built in their own type (midpoints and widths in C++
+    # integer arithmetic, wrapping where the reference's does), queried in
+    # float32; coordinates span the whole type so widths overflow
+    info = np.iinfo(dtype)
+    rng = np.random.default_rng(20 + dim)
+    P = rng.integers(info.min, info.max, (12_000, dim), dtype=dtype, endpoint=True)
+    P[:3000] = (P[:3000] // 64) * 3  # a dense clump with duplicates
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    assert t.dtype == np.dtype(dtype)
+    assert np.array_equal(t.reverse_indices(), o.reverse_indices())
+    assert np.array_equal(t.ref_nodes(), o.nodes())
+    gi, gc = gpu.kdtree.knn(t, None, 6)
+    oi, oc = o.knn_self(np.arange(len(P), dtype=np.int32), 6)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    q = P[rng.integers(0, len(P), 2000)].astype(np.float32) + np.float32(1.5)
+    gi, gc = gpu.kdtree.knn(t, q, 6)
+    oi, oc = o.knn(q, 6)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    r = float(np.float32(max(2.0, (float(info.max) - float(info.min)) / 4096)))
+    off, out = gpu.kdtree.rnear(t, q[:500], r)
+    ooff, oout = o.rnear(q[:500], r)
+    assert np.array_equal(off, ooff) and np.array_equal(out, oout)
+    # integer query arrays go through float32, one conversion per coordinate
+    qi = P[:300]
+    gi, gc = gpu.kdtree.knn(t, qi, 4)
+    oi, oc = o.knn(qi.astype(np.float32), 4)
+    assert np.array_equal(gi, oi)
+    # re-cutting the traversal hierarchy keeps every answer
+    t.set_bucket(16)
+    gi2, _ = gpu.kdtree.knn(t, qi, 4)
+    assert np.array_equal(gi2, gi)
+    # normals are defined for float32 / float64 points only
+    import ctypes
+    from pptk_b200 import _native as N
+    ev = np.empty((2, 3), np.float32)
+    with pytest.raises(TypeError):
+        N.call("pptkg_tree_normals", t._h, None, 2, N.MEM_HOST, 4, ctypes.c_float(np.inf), 1, 0, N.ptr(ev), None,
+               None, None)

@@ -34,7 +34,7 @@ def test_c_abi_rejects_bad_arguments_without_a_gpu():
     h = ctypes.c_void_p()
     assert lib.pptkg_tree_build(None, 10, 3, 0, N.MEM_HOST, 10, 0.2, None, ctypes.byref(h)) == N.E_INVALID
     assert lib.pptkg_tree_build(None, 0, 7, 0, N.MEM_HOST, 10, 0.2, None, ctypes.byref(h)) == N.E_TYPE
-    assert lib.pptkg_tree_build(None, 0, 3, 5, N.MEM_HOST, 10, 0.2, None, ctypes.byref(h)) == N.E_TYPE
+    assert lib.pptkg_tree_build(None, 0, 3, 11, N.MEM_HOST, 10, 0.2, None, ctypes.byref(h)) == N.E_TYPE
     assert lib.pptkg_knn(None, None, 0, 0, 0, 1, 1.0, None, None, None) == N.E_INVALID
     code, msg = N.last_error()
     assert code == N.E_INVALID and "null tree" in msg
@@ -103,8 +103,8 @@ def test_build_argument_checks_precede_device_work():
         kdtree._build("points")
     with pytest.raises(TypeError):
         kdtree._build(np.zeros((5, 3), np.float32), maxleafsize="x")
-    with pytest.raises(NotImplementedError):
-        kdtree._build(np.zeros((5, 3), np.int32))
+    with pytest.raises(RuntimeError, match="type_num"):
+        kdtree._build(np.zeros((5, 3), np.complex64))
 
 
 def test_synthetic_workloads_are_seeded():
