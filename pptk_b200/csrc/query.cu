@@ -177,6 +177,49 @@ __device__ __forceinline__ DistT seed_bound(const TreeView<T, D>& tv, const Dist
   return m01 < m2 ? m01 : m2;
 }
 
+// Tighter seed for float distances and k <= 16: the k-th smallest distance
+// from q to the 32 positions of [lo, hi) around `anchor` (`own` excluded),
+// sorted in registers by a bitonic network.  The window holds every window
+// of seed_bound, so this bound is never looser.  Infinity when fewer than k
+// candidates exist.
+template <typename T, int D>
+__device__ __forceinline__ float seed_bound32(const TreeView<T, D>& tv, const float* q, int anchor, int k, int own,
+                                             int lo, int hi) {
+  if (hi - lo < k + (own >= 0 ? 1 : 0) || anchor < 0) return INFINITY;
+  const int a = min(max(anchor, lo), hi - 1);
+  const int b = max(min(a - 16, hi - 32), lo);
+  float v[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int p = b + j;
+    v[j] = (p < hi && p != own) ? point_dist2<T, float, D>(tv.pts[p].c, q) : INFINITY;
+  }
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+    for (int stride = size / 2; stride > 0; stride >>= 1)
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const float x = v[i], y = v[j];
+          const float mn = fminf(x, y), mx = fmaxf(x, y);
+          if ((i & size) == 0) {
+            v[i] = mn;
+            v[j] = mx;
+          } else {
+            v[i] = mx;
+            v[j] = mn;
+          }
+        }
+      }
+  float r = INFINITY;
+#pragma unroll
+  for (int j = 0; j < 32; j++)
+    if (j == k - 1) r = v[j];
+  return r;
+}
+
 // Seeds a query's top-k bound from its neighbourhood in tree order.  Keeps a
 // warp of far-apart queries from visiting most of the tree before each
 // query's list fills up.
@@ -189,7 +232,12 @@ __device__ __forceinline__ void seed_topk(Top& top, const TreeView<T, D>& tv, co
     lo = (int)fm.valid_off[c];
     hi = (int)fm.valid_off[c + 1];
   }
-  top.seed(k, seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi), r2);
+  DistT b;
+  if constexpr (std::is_same<DistT, float>::value)
+    b = k <= 16 ? seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi) : seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
+  else
+    b = seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
+  top.seed(k, b, r2);
 }
 
 // order_mode 0: slot = query; 1: order[slot]; 2: tree order (query = the
@@ -319,8 +367,13 @@ int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaS
 }
 
 // ----------------------------------------------------------------- kNN ----
+// Blocks per SM the kNN kernel is compiled for: float top-k lists of up to
+// 16 entries fit 96 registers (5 blocks of 128 threads); larger lists keep
+// the compiler's register count.
+constexpr int knn_min_blocks(int kmax, int dist_bytes) { return (dist_bytes == 4 && kmax <= 16) ? 5 : 1; }
+
 template <typename T, int D, int KMAX, typename L>
-__global__ void __launch_bounds__(QTHREADS) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
+__global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename DistOf<T>::type))) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
                                                   int k, typename DistOf<T>::type r2, int32_t* out_idx,
                                                   int32_t* out_cnt, int* status, SlotMap fm, int lane_span) {
   typedef typename DistOf<T>::type DistT;
