@@ -68,7 +68,7 @@ def parse():
     p.add_argument("--points", type=int, default=20_000_000)
     p.add_argument("--k", type=int, default=16)
     p.add_argument("--slots", type=int, default=3)
-    p.add_argument("--max-batch", type=int, default=8_000_000, help="queries folded into one server batch")
+    p.add_argument("--max-batch", type=int, default=20_000_000, help="queries folded into one server batch")
     p.add_argument("--plain-sample", type=int, default=24, help="requests timed through the plain calls")
     p.add_argument("--latency-seconds", type=float, default=3.0)
     p.add_argument("--cpu-sample", type=int, default=1_000_000)

@@ -181,7 +181,7 @@ class Server:
     max_batch_queries: upper bound on the queries folded into one batch.
     """
 
-    def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=8_000_000, engine=None,
+    def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=20_000_000, engine=None,
                  fast_slots=1, small_batch=1_000_000):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)
