@@ -677,14 +677,17 @@ def run_serving_workload(args, ctx):
             del res
         return q / sum(lat), lat
 
-    plain_calls(mix[-2:], False, pts)
+    # warm-up: the largest request of each kind, so the device memory pool
+    # has grown to the sample's needs before the timed calls
+    warm = [max((r for r in sample if r[0] == kd), key=lambda r: len(r[1])) for kd in ("knn", "normals")]
+    plain_calls(warm, False, pts)
     plain_qps, plain_lat = plain_calls(sample, False, pts)
     plain = {"value": plain_qps, "unit": "queries/s", "latency": percentiles(plain_lat),
              "sample": f"first {len(sample)} requests of the stream ({sum(len(r) for _, r in sample)} queries), "
                        "one call each, device inputs"}
     if not args.no_e2e:
         host_pts = torch.from_numpy(pts).pin_memory().numpy()
-        plain_calls(mix[-2:], True, host_pts)
+        plain_calls(warm, True, host_pts)
         h_qps, h_lat = plain_calls(sample, True, host_pts)
         plain["e2e"] = {"value": h_qps, "unit": "queries/s", "latency": percentiles(h_lat),
                         "inputs": "host numpy (pinned scene); results returned as numpy"}

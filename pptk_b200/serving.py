@@ -179,13 +179,17 @@ class Server:
         last `fast_slots` of them run on high-priority streams and take the
         batches of at most `small_batch` queries first.
     max_batch_queries: upper bound on the queries folded into one batch.
+    max_host_batch_queries: the same bound for batches that return numpy
+        results: smaller batches let one batch's host copies overlap another
+        batch's kernels.
     """
 
     def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=20_000_000, engine=None,
-                 fast_slots=1, small_batch=1_000_000):
+                 fast_slots=1, small_batch=1_000_000, max_host_batch_queries=8_000_000):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)
         self.max_batch = int(max_batch_queries)
+        self.max_host_batch = int(max_host_batch_queries)
         self.small_batch = int(small_batch)
         self.trees = {}
         self.tree_bytes = {}
@@ -266,6 +270,7 @@ class Server:
         into one batch up to max_batch_queries."""
         out = []
         queries = 0
+        host = False
         while self._pending:
             r = self._pending[0]
             if r.kind != "build" and r.args[0] not in self.trees:
@@ -273,7 +278,9 @@ class Server:
                 r.future.set_exception(KeyError(f"unknown tree {r.args[0]}"))
                 continue
             exclusive = r.kind in ("build", "rnear")
-            if out and (exclusive or queries + r.m > self.max_batch):
+            r_host = bool(r.key and r.key[-1] is True)
+            cap = self.max_host_batch if (host or r_host) else self.max_batch
+            if out and (exclusive or queries + r.m > cap):
                 break
             if self._committed + r.bytes > self.budget:
                 break
@@ -281,6 +288,7 @@ class Server:
             self._committed += r.bytes
             out.append(r)
             queries += r.m
+            host = host or r_host
             if exclusive:
                 break
         return out
