@@ -64,7 +64,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="serving", choices=["serving", "plain", "ragged", "multitree"])
+    p.add_argument("--workload", default="serving", choices=["serving", "plain", "ragged", "multitree", "scene"])
     p.add_argument("--points", type=int, default=20_000_000)
     p.add_argument("--k", type=int, default=16)
     p.add_argument("--slots", type=int, default=3)
@@ -576,6 +576,84 @@ def run_multitree_workload(args, ctx):
             "e2e": None, "gpu_launches": None, "roofline": None, "cpu_baseline": None, "clocks": clk}
 
 
+def run_scene_workload(args, ctx):
+    """The 20M-point scene's other queries (config 2): kNN k=32 for every
+    point (self queries, tree order), r-near r=0.5 m hit counts for every
+    point, and the r-near hit lists for 20k random points (filling them for
+    every point is not feasible on any machine: a point within ~1 m of the
+    sensor has ~1e5 hits at r=0.5 m, about a tenth of the points lie there).
+    `value` is the kNN k=32 rate; the r-near figures sit beside it."""
+    torch, N = ctx.torch, ctx.N
+    from pptk_b200 import kdtree, synth
+    pts = synth.lidar_scene(args.points, seed=2)
+    n = len(pts)
+    dev = torch.from_numpy(pts).cuda()
+    tree = kdtree._build(dev)
+    k = 32
+    idx = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    cnt = torch.empty((n,), dtype=torch.int32, device="cuda")
+    sp = N.torch_stream()
+
+    def knn_step():
+        N.call("pptkg_knn_self", tree._h, None, n, N.MEM_DEVICE, k, float("inf"), N.ptr(idx), N.ptr(cnt), sp)
+
+    for _ in range(args.warmup):
+        knn_step()
+    ctx.lib.pptkg_profile_enable(1)
+    ms, launches, clk = device_timed(ctx, knn_step, args.steps)
+    ctx.lib.pptkg_profile_enable(0)
+    ms_max = ctx.max_over_ranks(ms)
+    value = ctx.throughput(n, ms / 1e3)
+    # r-near counts for every point (the count pass of count / scan / fill)
+    r = 0.5
+    off = torch.empty((n + 1,), dtype=torch.int64, device="cuda")
+    total = ctypes.c_int64()
+
+    def count_step():
+        N.call("pptkg_rnear_count", tree._h, None, None, n, 0, N.MEM_DEVICE, r, N.ptr(off), ctypes.byref(total), sp)
+
+    count_step()
+    ms_c, _, _ = device_timed(ctx, count_step, args.steps)
+    hits = int(total.value)
+    # hit lists for a sample
+    rows = torch.from_numpy(np.random.default_rng(13).integers(0, n, 20_000).astype(np.int32)).cuda()
+    q = dev[rows.long()].contiguous()
+
+    def sample_step():
+        return kdtree.rnear(tree, q, r)
+
+    sample_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o_, h_ = sample_step()
+    torch.cuda.synchronize()
+    ms_s = (time.perf_counter() - t0) / args.steps * 1e3
+    sample_hits = int(o_[-1].item())
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        sel = np.sort(np.random.default_rng(0).choice(n, size=1_000_000, replace=False))
+        ref = O.RefTree(np.ascontiguousarray(pts[sel])) if O.ref_available() else O.PortTree(
+            np.ascontiguousarray(pts[sel]))
+        t0 = time.perf_counter()
+        ref.knn_self(np.arange(len(sel), dtype=np.int32), k, nthreads=0)
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sel) / dt, "unit": "queries/s", "cores": O.ref_lib().ref_max_threads(),
+               "kind": "reference" if O.ref_available() else "port",
+               "sample": f"kNN k={k} self queries over a 1M-point random sample of the scene (tree built beforehand, "
+                         f"{dt:.1f} s)"}
+    return {"value": value, "ms_per_step": ms_max,
+            "config": {"workload": f"lidar_scene_{n}_f32: kNN k={k} self queries for every point (tree order)",
+                       "points": n, "k": k, "parallelism": f"replicas x{ctx.world}"},
+            "rnear": {"r": r, "count_all_points_ms": ms_c, "count_queries_per_s": n / (ms_c / 1e3),
+                      "total_hits_all_points": hits,
+                      "sample_queries": 20_000, "sample_hits": sample_hits, "sample_count_and_fill_ms": ms_s,
+                      "note": "hit lists for all points would be "
+                              f"{hits * 4 / 1e9:.0f} GB; filled for a 20k-point sample only"},
+            "e2e": None, "gpu_launches": launches, "roofline": None, "cpu_baseline": cpu, "clocks": clk}
+
+
 def percentiles(lat_s):
     a = np.asarray(lat_s, dtype=np.float64) * 1e3
     return {"p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)), "requests": int(a.size)}
@@ -786,7 +864,8 @@ def run_ours(args):
     ctx.lib.pptkg_profile_enable.argtypes = [ctypes.c_int]
     ctx.lib.pptkg_launch_count.restype = ctypes.c_int64
     res = {"serving": run_serving_workload, "plain": run_plain_workload,
-           "ragged": run_ragged_workload, "multitree": run_multitree_workload}[args.workload](args, ctx)
+           "ragged": run_ragged_workload, "multitree": run_multitree_workload,
+           "scene": run_scene_workload}[args.workload](args, ctx)
     if ctx.rank == 0 and ctx.world == 1 and not args.no_precision:
         res["precision"] = precision_report()
     if ctx.rank == 0:

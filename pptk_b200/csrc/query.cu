@@ -370,7 +370,7 @@ int make_order(const TreeBase* t, const QuerySpec& qs, DevBuf<int>& order, cudaS
 // Blocks per SM the kNN kernel is compiled for: float top-k lists of up to
 // 16 entries fit 96 registers (5 blocks of 128 threads); larger lists keep
 // the compiler's register count.
-constexpr int knn_min_blocks(int kmax, int dist_bytes) { return (dist_bytes == 4 && kmax <= 16) ? 5 : 1; }
+constexpr int knn_min_blocks(int kmax, int dist_bytes) { return (dist_bytes == 4 && kmax <= 16) ? 5 : (dist_bytes == 4 && kmax <= 32) ? 4 : 1; }
 
 template <typename T, int D, int KMAX, typename L>
 __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename DistOf<T>::type))) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
