@@ -231,6 +231,17 @@ PPTKG_API int pptkg_eigh3(const void* A, int64_t m, int dtype, int mem, void* w,
 PPTKG_API int pptkg_nbhd_covariance(const void* points, int64_t n, int dtype, int mem, const int64_t* offsets,
                                    const int32_t* indices, int64_t m, void* out_cov, void* stream);
 
+/* Tree persistence (no reference counterpart: the reference keeps trees in
+ * process memory only).  pptkg_tree_save writes a tree or forest to one
+ * self-describing host buffer (header, the device arrays, a checksum);
+ * with buf NULL it only reports the size.  pptkg_tree_load puts such a
+ * buffer back on the current device without a rebuild; the header, sizes,
+ * checksum and records are checked on the host and every node reference,
+ * point id and index-map entry on the device, so a damaged buffer is
+ * PPTKG_E_INVALID. */
+PPTKG_API int pptkg_tree_save(const pptkg_tree* tree, void* buf, int64_t capacity, int64_t* size);
+PPTKG_API int pptkg_tree_load(const void* buf, int64_t size, void* stream, pptkg_tree** out);
+
 /* Instrumentation (no reference counterpart).  Stage timing records CUDA
  * events on the launching stream around each stage ("build", "order",
  * "knn", "normals", "rnear_count", "rnear_fill", "h2d", "d2h");

@@ -68,6 +68,8 @@ SIGNATURES = {
     "pptkg_tune_set": [ctypes.c_char_p, _i64],
     "pptkg_tune_get": [ctypes.c_char_p, _pi64],
     "pptkg_set_status_sink": [_vp],
+    "pptkg_tree_save": [_vp, _vp, _i64, _pi64],
+    "pptkg_tree_load": [_vp, _i64, _vp, _pvp],
 }
 
 _lib = None

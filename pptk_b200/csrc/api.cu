@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "build.cuh"
+#include "persist.cuh"
 #include "pptkg.h"
 #include "profile.cuh"
 #include "query.cuh"
@@ -738,6 +739,30 @@ int pptkg_nbhd_covariance(const void* points, int64_t n, int dtype, int mem, con
       c.flush(S(stream));
       PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
     });
+  });
+}
+
+int pptkg_tree_save(const pptkg_tree* tree, void* buf, int64_t capacity, int64_t* size) {
+  return guarded([&] {
+    const TreeBase* t = tree_of(tree);
+    DeviceGuard g(t->device);
+    std::vector<char> blob = save_tree(t, t->stream);
+    if (size) *size = (int64_t)blob.size();
+    if (buf) {
+      if (capacity < (int64_t)blob.size()) throw Error(E_INVALID, "buffer too small for the stored tree");
+      memcpy(buf, blob.data(), blob.size());
+    }
+  });
+}
+
+int pptkg_tree_load(const void* buf, int64_t size, void* stream, pptkg_tree** out) {
+  return guarded([&] {
+    if (!out) throw Error(E_INVALID, "out is null");
+    *out = nullptr;
+    if (size < 0) throw Error(E_INVALID, "negative size");
+    std::unique_ptr<pptkg_tree> h(new pptkg_tree());
+    h->t.reset(load_tree((const char*)buf, (size_t)size, S(stream)));
+    *out = h.release();
   });
 }
 

@@ -850,10 +850,6 @@ __global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncloud) return;
   const int r = root_rec[c];
-  if (r >= 0 && flag[r]) {
-    root_tnode[c] = tid[r];
-    return;
-  }
   TNode<T, D> t;
   for (int k = 0; k < 2; k++)
     for (int d = 0; d < D; d++) {
@@ -862,6 +858,13 @@ __global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64
     }
   t.ref[0] = t.ref[1] = -1;
   t.cnt[0] = t.cnt[1] = 0;
+  if (r >= 0 && flag[r]) {
+    // the root record has its own node; the reserved slot stays an empty
+    // node (nothing refers to it, but every slot holds a well-formed node)
+    nodes[nt + c] = t;
+    root_tnode[c] = tid[r];
+    return;
+  }
   if (r >= 0) {
     for (int d = 0; d < D; d++) {
       t.lo[0][d] = recs[r].lo[d];

@@ -47,6 +47,11 @@ class KdTree:
                 pass
             self._h = None
 
+    def save(self, path):
+        """Writes the device tree to `path` (pptkg_tree_save); kdtree.load
+        puts it back on a device without rebuilding."""
+        _save_handle(self._h, path)
+
     def num_points(self):
         """Number of stored (valid) points, the reference's num_points()."""
         return self.n_valid
@@ -307,3 +312,31 @@ def _query(kdtree, queries, k=_UNSET, dmax=_UNSET, numprocs=-1):
         o = off.tolist() if isinstance(off, np.ndarray) else off.cpu().tolist()
         return [out[o[i]:o[i + 1]] for i in range(b.m)]
     raise ValueError(f"{form}: k = {kk} and dmax = {dm:f} is an invalid combination.")
+
+
+def _save_handle(h, path):
+    size = ctypes.c_int64()
+    N.call("pptkg_tree_save", h, None, 0, ctypes.byref(size), where="save()")
+    buf = np.empty(size.value, np.uint8)
+    N.call("pptkg_tree_save", h, N.ptr(buf), size.value, ctypes.byref(size), where="save()")
+    with open(path, "wb") as f:
+        f.write(buf.tobytes())
+
+
+def _load_handle(path, device=None):
+    data = np.fromfile(path, dtype=np.uint8)
+    h = ctypes.c_void_p()
+    if device is not None:
+        import torch
+        with torch.cuda.device(device):
+            N.call("pptkg_tree_load", N.ptr(data), data.size, None, ctypes.byref(h), where="load()")
+    else:
+        N.call("pptkg_tree_load", N.ptr(data), data.size, None, ctypes.byref(h), where="load()")
+    return h
+
+
+def load(path, device=None):
+    """A KdTree read back from a file written by KdTree.save, on `device`
+    (a CUDA device index or torch.device; default: the current device).
+    Damaged files raise ValueError."""
+    return KdTree(_load_handle(path, device), device)

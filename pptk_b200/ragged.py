@@ -90,6 +90,52 @@ class Forest:
         N.call("pptkg_forest_ref_nodes", self._h, int(cloud), N.ptr(out), cnt.value, ctypes.byref(cnt))
         return out
 
+    def save(self, path):
+        """Writes the forest to `path`; Forest.load reads it back."""
+        from .kdtree import _save_handle
+        _save_handle(self._h, path)
+
+    @classmethod
+    def load(cls, path, offsets, device=None, torch_results=None):
+        """A forest read back from Forest.save.  `offsets` are the clouds'
+        input offsets (checked against the stored ones).  Results come back
+        as CUDA tensors when torch_results (default: device given)."""
+        from .kdtree import _load_handle
+        self = cls.__new__(cls)
+        self._h = _load_handle(path, device)
+        nc = ctypes.c_int()
+        N.call("pptkg_forest_info", self._h, ctypes.byref(nc), None)
+        vo = np.empty(nc.value + 1, np.int64)
+        N.call("pptkg_forest_info", self._h, ctypes.byref(nc), N.ptr(vo))
+        off = np.asarray(offsets, dtype=np.int64)
+        if off.size != nc.value + 1:
+            raise ValueError("offsets do not match the stored forest")
+        n = ctypes.c_int64()
+        nv = ctypes.c_int64()
+        dim = ctypes.c_int()
+        dt = ctypes.c_int()
+        nrec = ctypes.c_int64()
+        depth = ctypes.c_int()
+        N.call("pptkg_tree_info", self._h, ctypes.byref(n), ctypes.byref(nv), ctypes.byref(dim), ctypes.byref(dt),
+               ctypes.byref(nrec), ctypes.byref(depth))
+        if off[-1] != n.value:
+            raise ValueError("offsets do not match the stored forest")
+        self.n, self.dim = n.value, dim.value
+        self.dtype = N.CODE_DTYPES[dt.value]
+        self.offsets = off
+        self.ncloud = nc.value
+        self.valid_offsets = vo
+        self.n_valid = int(vo[-1])
+        self._torch = (device is not None) if torch_results is None else bool(torch_results)
+        if self._torch:
+            import torch
+            self.device = torch.device("cuda", device if isinstance(device, int) else
+                                       (torch.cuda.current_device() if device is None else torch.device(device).index))
+            self._stream = N.torch_stream(self.device)
+        else:
+            self.device, self._stream = None, None
+        return self
+
     def set_bucket(self, bucket):
         N.call("pptkg_tree_set_bucket", self._h, int(bucket), self._stream)
 
