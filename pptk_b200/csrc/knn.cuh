@@ -418,6 +418,67 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
   }
 }
 
+// Top-k of any size k for the per-lane walk: a binary max-heap of
+// (dist2, position) pairs in device memory, ordered like the register lists
+// ((dist2, position) lexicographic), so the k kept are the same k smallest.
+// Slot 0 holds the current k-th once the heap is full.
+template <typename DistT>
+struct HeapTop {
+  DistT* d;
+  int* p;
+  int k, size;
+  DistT r2;
+  __device__ __forceinline__ static bool gt(DistT da, int pa, DistT db, int pb) {
+    return da > db || (da == db && pa > pb);
+  }
+  __device__ __forceinline__ DistT worst() const { return size < k ? r2 : d[0]; }
+  __device__ void sift_down(int i, int n) {
+    const DistT di = d[i];
+    const int pi = p[i];
+    while (true) {
+      int c = 2 * i + 1;
+      if (c >= n) break;
+      if (c + 1 < n && gt(d[c + 1], p[c + 1], d[c], p[c])) c++;
+      if (!gt(d[c], p[c], di, pi)) break;
+      d[i] = d[c];
+      p[i] = p[c];
+      i = c;
+    }
+    d[i] = di;
+    p[i] = pi;
+  }
+  __device__ void offer(DistT d2, int pos) {
+    if (size < k) {
+      int i = size++;
+      while (i > 0) {
+        const int par = (i - 1) / 2;
+        if (!gt(d2, pos, d[par], p[par])) break;
+        d[i] = d[par];
+        p[i] = p[par];
+        i = par;
+      }
+      d[i] = d2;
+      p[i] = pos;
+    } else if (gt(d[0], p[0], d2, pos)) {
+      d[0] = d2;
+      p[0] = pos;
+      sift_down(0, size);
+    }
+  }
+  // Sorts the kept pairs ascending in place (heap sort).
+  __device__ void sort() {
+    for (int e = size - 1; e > 0; e--) {
+      const DistT td = d[0];
+      const int tp = p[0];
+      d[0] = d[e];
+      p[0] = p[e];
+      d[e] = td;
+      p[e] = tp;
+      sift_down(0, e);
+    }
+  }
+};
+
 // Warp-uniform choice of the traversal: per-lane walks when the warp's
 // queries span more than `span` tree positions (anchors: tree positions near
 // each query; -1 unknown), packet walks otherwise.

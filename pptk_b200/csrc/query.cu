@@ -479,12 +479,53 @@ struct StatusWord {
 };
 
 
+// kNN for k above the register lists' capacity: one thread per query, the
+// per-lane walk with its top-k in a device-memory heap (HeapTop), then a heap
+// sort into ascending order.  Queries run in chunks of `m` slots starting
+// at slot `m0` of the processing order; hd / hp hold one heap per slot.
+constexpr int BIG_STACK = 128;
+
+template <typename T, int D, typename L>
+__global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m0, int m, int k,
+                          typename DistOf<T>::type r2, typename DistOf<T>::type* hd, int* hp, int32_t* out_idx,
+                          int32_t* out_cnt, int* status) {
+  typedef typename DistOf<T>::type DistT;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int qid = query_of(m0 + i, order, order_mode, tv);
+  int own = -1;
+  DistT q[D];
+  const bool active = ld.load(qid, tv, q, own);
+  HeapTop<DistT> top{hd + (int64_t)i * k, hp + (int64_t)i * k, k, 0, r2};
+  if (active && !lane_knn<BIG_STACK, T, D>(tv, q, own, true, r2, top)) atomicExch(status, 1);
+  top.sort();
+  int32_t* out = out_idx + (int64_t)qid * k;
+  for (int j = 0; j < k; j++) out[j] = j < top.size ? tv.pts[top.p[j]].id : -1;
+  if (out_cnt) out_cnt[qid] = top.size;
+}
+
+template <typename T, int D, typename L>
+void launch_knn_big(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                    int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (t->tdepth > BIG_STACK) throw Error(E_UNSUPPORTED, "k > 64 on a tree deeper than 128 levels");
+  const size_t per_query = (size_t)k * (sizeof(DistT) + sizeof(int));
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)m, ((size_t)2 << 30) / per_query));
+  DevBuf<DistT> hd((size_t)chunk * k, st);
+  DevBuf<int> hp((size_t)chunk * k, st);
+  for (int m0 = 0; m0 < m; m0 += chunk) {
+    const int mc = std::min(chunk, m - m0);
+    k_knn_big<T, D, L><<<div_up(mc, 128), 128, 0, st>>>(view_of<T, D>(t), ld, order, mode, m0, mc, k, r2, hd.get(),
+                                                          hp.get(), d_idx, d_cnt, status);
+    PPTKG_CHECK_LAUNCH();
+  }
+}
+
 template <typename T, int D>
 void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32_t* d_idx, int32_t* d_cnt,
                cudaStream_t st) {
   typedef typename DistOf<T>::type DistT;
   if (k < 1) throw Error(E_INVALID, "k must be positive");
-  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU kNN kernels");
   const int m = (int)qs.m;
   if (m <= 0) return;
   DevBuf<int> status(1, st);
@@ -493,6 +534,24 @@ void knn_query(const TreeBase* t, const QuerySpec& qs, int k, double dmax, int32
   const int mode = make_order<T, D>(t, qs, order, st, false, anchors.get());
   const DistT r2 = radius2<DistT>(dmax);
   Stage stage("knn", st);
+  if (k > KNN_MAX_K) {
+    if (qs.pts) {
+      if (qs.qdtype == F64)
+        launch_knn_big<T, D>(t, PointQueries<double, D>{(const double*)qs.pts}, order.get(), mode, m, k, r2, d_idx,
+                             d_cnt, status.get(), st);
+      else
+        launch_knn_big<T, D>(t, PointQueries<float, D>{(const float*)qs.pts}, order.get(), mode, m, k, r2, d_idx,
+                             d_cnt, status.get(), st);
+    } else if (qs.exclude_self) {
+      launch_knn_big<T, D>(t, IndexQueries<D, true>{qs.idx, t->fwd}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                           status.get(), st);
+    } else {
+      launch_knn_big<T, D>(t, IndexQueries<D, false>{qs.idx, t->fwd}, order.get(), mode, m, k, r2, d_idx, d_cnt,
+                           status.get(), st);
+    }
+    check_status(status.get(), st, "knn");
+    return;
+  }
   if (qs.pts) {
     if (qs.qdtype == F64)
       dispatch_knn<T, D>(t, PointQueries<double, D>{(const double*)qs.pts, anchors.get()}, order.get(), mode, m, k,

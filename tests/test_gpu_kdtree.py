@@ -303,3 +303,25 @@ def test_integer_trees_match_oracle(gpu, port, dtype, dim):
     with pytest.raises(TypeError):
         N.call("pptkg_tree_normals", t._h, None, 2, N.MEM_HOST, 4, ctypes.c_float(np.inf), 1, 0, N.ptr(ev), None,
                None, None)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_large_k_matches_oracle(gpu, port, dtype):
+    # k above the register lists' capacity (64): device-memory heaps
+    rng = np.random.default_rng(30)
+    P = rng.random((30_000, 3)).astype(dtype)
+    P[::211] = P[1::211]  # duplicates (distance ties)
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    for k in (65, 100, 257):
+        gi, gc = gpu.kdtree.knn(t, None, k)
+        oi, oc = o.knn_self(np.arange(len(P), dtype=np.int32), k)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi), k
+    q = rng.random((4000, 3)).astype(dtype)
+    gi, gc = gpu.kdtree.knn(t, q, 130, dmax=0.1)
+    oi, oc = o.knn(q, 130, dmax=float(np.float32(0.1)))
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi)
+    assert (gc < 130).any() and (gc == 130).any()  # dmax cuts some lists short
+    rows = gpu.kdtree._query(t, q[:20], k=200)
+    ei, _ = o.knn(q[:20], 200)
+    assert all(np.array_equal(a, b) for a, b in zip(rows, ei))
