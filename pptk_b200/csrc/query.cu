@@ -485,7 +485,9 @@ struct StatusWord {
 // at slot `m0` of the processing order; hd / hp hold one heap per slot.
 constexpr int BIG_STACK = 128;
 
-template <typename T, int D, typename L>
+// POS: write tree positions to chunk rows (for the normal pass) instead of
+// original indices to query rows.
+template <typename T, int D, typename L, bool POS>
 __global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m0, int m, int k,
                           typename DistOf<T>::type r2, typename DistOf<T>::type* hd, int* hp, int32_t* out_idx,
                           int32_t* out_cnt, int* status) {
@@ -499,9 +501,10 @@ __global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_m
   HeapTop<DistT> top{hd + (int64_t)i * k, hp + (int64_t)i * k, k, 0, r2};
   if (active && !lane_knn<BIG_STACK, T, D>(tv, q, own, true, r2, top)) atomicExch(status, 1);
   top.sort();
-  int32_t* out = out_idx + (int64_t)qid * k;
-  for (int j = 0; j < k; j++) out[j] = j < top.size ? tv.pts[top.p[j]].id : -1;
-  if (out_cnt) out_cnt[qid] = top.size;
+  const int64_t row = POS ? i : qid;
+  int32_t* out = out_idx + row * k;
+  for (int j = 0; j < k; j++) out[j] = j < top.size ? (POS ? top.p[j] : tv.pts[top.p[j]].id) : -1;
+  if (out_cnt) out_cnt[row] = top.size;
 }
 
 template <typename T, int D, typename L>
@@ -515,8 +518,8 @@ void launch_knn_big(const TreeBase* t, L ld, const int* order, int mode, int m, 
   DevBuf<int> hp((size_t)chunk * k, st);
   for (int m0 = 0; m0 < m; m0 += chunk) {
     const int mc = std::min(chunk, m - m0);
-    k_knn_big<T, D, L><<<div_up(mc, 128), 128, 0, st>>>(view_of<T, D>(t), ld, order, mode, m0, mc, k, r2, hd.get(),
-                                                          hp.get(), d_idx, d_cnt, status);
+    k_knn_big<T, D, L, false><<<div_up(mc, 128), 128, 0, st>>>(view_of<T, D>(t), ld, order, mode, m0, mc, k, r2,
+                                                                 hd.get(), hp.get(), d_idx, d_cnt, status);
     PPTKG_CHECK_LAUNCH();
   }
 }
@@ -1001,12 +1004,84 @@ void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m
     normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
 }
 
+// Normals of neighbourhoods held as tree positions (pos: m x k, counts cnt),
+// the large-k path: float64 covariance shifted to the query point and
+// centred, float64 eigensolve, results in T.
+template <typename T, typename L>
+__global__ void k_normals_pos(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m0, int m, int k,
+                              const int32_t* pos, const int32_t* cnt, int num_eigen, T* evecs, T* evals,
+                              int32_t* sizes) {
+  typedef typename DistOf<T>::type DistT;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int qid = query_of(m0 + i, order, order_mode, tv);
+  int own = -1;
+  DistT q[3];
+  const bool active = ld.load(qid, tv, q, own);
+  const int n = cnt[i];
+  if (!active || n <= 0) {
+    write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
+    return;
+  }
+  const int32_t* P = pos + (int64_t)i * k;
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> rp = tv.pts[P[j]];
+    s0 += (double)rp.c[0] - (double)q[0];
+    s1 += (double)rp.c[1] - (double)q[1];
+    s2 += (double)rp.c[2] - (double)q[2];
+  }
+  const double inv = 1.0 / (double)n, a0 = s0 * inv, a1 = s1 * inv, a2 = s2 * inv;
+  Sym3<double> C{0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < n; j++) {
+    const PointRec<T, 3> rp = tv.pts[P[j]];
+    const double x = (double)rp.c[0] - (double)q[0] - a0, y = (double)rp.c[1] - (double)q[1] - a1,
+                 z = (double)rp.c[2] - (double)q[2] - a2;
+    C.a00 += x * x;
+    C.a01 += x * y;
+    C.a02 += x * z;
+    C.a11 += y * y;
+    C.a12 += y * z;
+    C.a22 += z * z;
+  }
+  C.a00 *= inv;
+  C.a01 *= inv;
+  C.a02 *= inv;
+  C.a11 *= inv;
+  C.a12 *= inv;
+  C.a22 *= inv;
+  double w[3], V[9];
+  eigh3<double>(C, w, V);
+  write_pca<T, double>(qid, n, w, V, num_eigen, evecs, evals, sizes);
+}
+
+// estimate_normals with k above the register lists: the large-k walk writes
+// each chunk's neighbourhoods as tree positions, k_normals_pos solves them.
+template <typename T, typename L>
+void normals_big(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
+                 int num_eigen, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st) {
+  typedef typename DistOf<T>::type DistT;
+  if (t->tdepth > BIG_STACK) throw Error(E_UNSUPPORTED, "k > 64 on a tree deeper than 128 levels");
+  const size_t per_query = (size_t)k * (sizeof(DistT) + 2 * sizeof(int)) + sizeof(int);
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)m, ((size_t)2 << 30) / per_query));
+  DevBuf<DistT> hd((size_t)chunk * k, st);
+  DevBuf<int> hp((size_t)chunk * k, st), pos((size_t)chunk * k, st), cnt(chunk, st);
+  for (int m0 = 0; m0 < m; m0 += chunk) {
+    const int mc = std::min(chunk, m - m0);
+    k_knn_big<T, 3, L, true><<<div_up(mc, 128), 128, 0, st>>>(view_of<T, 3>(t), ld, order, mode, m0, mc, k, r2,
+                                                                hd.get(), hp.get(), pos.get(), cnt.get(), status);
+    PPTKG_CHECK_LAUNCH();
+    k_normals_pos<T, L><<<div_up(mc, 128), 128, 0, st>>>(view_of<T, 3>(t), ld, order, mode, m0, mc, k, pos.get(),
+                                                          cnt.get(), num_eigen, ev, ew, sz);
+    PPTKG_CHECK_LAUNCH();
+  }
+}
+
 template <typename T>
 void normals_query(const TreeBase* t, const QuerySpec& qs_in, int k, float r, int num_eigen, int precision,
                    double gap_thr, T* d_evecs, T* d_evals, int32_t* d_sizes, cudaStream_t st) {
   typedef typename DistOf<T>::type DistT;
   if (k == 0 || k < -1) throw Error(E_INVALID, "k must be positive or -1");
-  if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU normal kernels");
   QuerySpec qs = qs_in;
   qs.pts = nullptr;
   qs.exclude_self = false;
@@ -1034,6 +1109,9 @@ void normals_query(const TreeBase* t, const QuerySpec& qs_in, int k, float r, in
     k_normals_rnear<T, IndexQueries<3, false>><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
         view_of<T, 3>(t), ld, order.get(), mode, m, r2, num_eigen, d_evecs, d_evals, d_sizes, status.get());
     PPTKG_CHECK_LAUNCH();
+  } else if (k > KNN_MAX_K) {
+    normals_big<T, IndexQueries<3, false>>(t, ld, order.get(), mode, m, k, r2, num_eigen, d_evecs, d_evals, d_sizes,
+                                          status.get(), st);
   } else {
     int prec = precision;
     if (prec == PREC_AUTO) prec = sizeof(T) == 4 ? PREC_FP32 : PREC_FP64;

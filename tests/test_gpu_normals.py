@@ -163,3 +163,15 @@ def test_eigh3_batched(gpu):
         assert (np.abs((V * Vl).sum(1))[ok] > 1 - 100 * tol).all()
         w2, V2 = gpu.eigh3(A.astype(dt), layout="rows")
         assert np.array_equal(V2, np.transpose(V, (0, 2, 1)))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_large_k_normals_match_fp64_oracle(gpu, port, dtype):
+    # k above the register lists (64): device-memory heaps, FP64 covariance
+    P = np.random.default_rng(7).random((30_000, 3)).astype(dtype)
+    P[:, 2] *= 0.1
+    for k, r in ((100, np.inf), (150, 0.08)):
+        out = gpu.estimate_normals(P, k, r, output_eigenvalues=True, output_all_eigenvectors=True,
+                                   output_neighborhood_sizes=True, verbose=False)
+        excluded, ang = _check_against_fp64(port, P, k, r, out, f"{dtype} k={k}")
+        assert excluded < len(P) * 1e-3
