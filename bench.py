@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 angular error report")
+    p.add_argument("--tune", action="append", default=[], metavar="NAME=VALUE",
+                   help="a traversal knob applied before the run (pptkg_tune_set), e.g. lane_span=64")
     return p.parse_args()
 
 
@@ -861,6 +863,11 @@ def precision_report():
 
 def run_ours(args):
     ctx = Ctx()
+    tuned = {}
+    for kv in args.tune:
+        name, val = kv.split("=", 1)
+        ctx.N.tune_set(name, int(val))
+        tuned[name] = int(val)
     ctx.lib.pptkg_profile_enable.argtypes = [ctypes.c_int]
     ctx.lib.pptkg_launch_count.restype = ctypes.c_int64
     res = {"serving": run_serving_workload, "plain": run_plain_workload,
@@ -874,6 +881,8 @@ def run_ours(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic"}
         line.update(res)
+        if tuned:
+            line["config"]["tune"] = tuned
         print(json.dumps(line), flush=True)
     ctx.finish()
 

@@ -258,7 +258,7 @@ __global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
   for (int d = 0; d < D; d++) p[d] = (DistT)q[(int64_t)i * D + d];
   int cur = tv.root, k = 0;
   for (int step = 0; step <= tv.depth + 1; step++) {
-    const TNode<T, D>& nd = tv.nodes[cur];
+    const TNode<T, D> nd = load_node(tv.nodes, cur);
     int c;
     if (nd.cnt[1] == 0)
       c = 0;
