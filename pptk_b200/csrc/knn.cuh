@@ -164,6 +164,33 @@ struct WarpScratch {
   typename DistOf<T>::type* dmat;        // 32 x 33 distances (kNN bucket scan); null when unused
 };
 
+// A lane's query as the rest of its warp reads it during a bucket scan:
+// the coordinates and the entry bound (a candidate enters the list iff its
+// dist2 <= thr).
+template <typename DistT, int D>
+struct alignas(16) QStage {
+  DistT q[D];
+  DistT thr;
+};
+
+// The largest value below r2 (r2 > 0), -1 for r2 <= 0, so that for every
+// distance d2 >= 0: d2 < r2  <=>  d2 <= below(r2).
+__device__ __forceinline__ float below(float r2) {
+  if (!(r2 > 0.f)) return -1.f;
+  return __uint_as_float(__float_as_uint(r2) - 1u);  // +inf -> FLT_MAX
+}
+__device__ __forceinline__ double below(double r2) {
+  if (!(r2 > 0.0)) return -1.0;
+  return __longlong_as_double(__double_as_longlong(r2) - 1ll);  // +inf -> DBL_MAX
+}
+
+// Entry bound of a list whose k-th distance is `worst` (worst <= r2 always):
+// d2 <= entry_bound  <=>  d2 <= worst && d2 < r2.
+template <typename DistT>
+__device__ __forceinline__ DistT entry_bound(DistT worst, DistT r2_below) {
+  return worst < r2_below ? worst : r2_below;
+}
+
 // One deferred child on the per-warp traversal stack: its box travels with
 // it, so a pop re-tests the box from shared memory without touching the node
 // array.  ref >= 0: inner node; ref < 0: leaf bucket starting at -ref - 1.
@@ -209,6 +236,12 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
   // candidate's distance to q_i; the row goes to dmat[i][*] and the ballot of
   // candidates that can enter list i becomes lane i's mark mask.  Each lane
   // then inserts its marked candidates, reading distances from its row.
+  // The queries sit in the warp's staging buffer (unused by kNN walks) so
+  // that lane i's coordinates and bound arrive as one shared broadcast.
+  QStage<DistT, D>* qst = reinterpret_cast<QStage<DistT, D>*>(ws.buf);
+  const DistT r2_below = below(r2);
+#pragma unroll
+  for (int d = 0; d < D; d++) qst[lane].q[d] = q[d];
   auto scan = [&](int begin, int count, bool mine) {
     const unsigned needm = __ballot_sync(FULL, mine);
     for (int base = begin; base < begin + count; base += 32) {
@@ -220,22 +253,25 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
 #pragma unroll
         for (int d = 0; d < D; d++) pr.c[d] = (T)0;
       }
-      const DistT thr_mine = top.worst();
+      // each needing lane publishes its entry bound for this chunk; the
+      // loop below reads a query and its bound as one broadcast
+      __syncwarp();
+      qst[lane].thr = entry_bound(top.worst(), r2_below);
+      __syncwarp();
+      const unsigned valid = nb == 32 ? FULL : (1u << nb) - 1u;
       unsigned mark = 0;
       unsigned rem = needm;
       while (rem) {
         const int i = __ffs(rem) - 1;
         rem &= rem - 1;
-        DistT qi[D];
-#pragma unroll
-        for (int d = 0; d < D; d++) qi[d] = __shfl_sync(FULL, q[d], i);
-        const DistT thr = __shfl_sync(FULL, thr_mine, i);
-        const int own_i = __shfl_sync(FULL, own, i);
-        const DistT d2 = point_dist2<T, DistT, D>(pr.c, qi);
+        const QStage<DistT, D> qi = qst[i];
+        const DistT d2 = point_dist2<T, DistT, D>(pr.c, qi.q);
         ws.dmat[i * 33 + lane] = d2;
-        const unsigned m = __ballot_sync(FULL, lane < nb && d2 <= thr && d2 < r2 && base + lane != own_i);
+        const unsigned m = __ballot_sync(FULL, d2 <= qi.thr) & valid;
         if (lane == i) mark = m;
       }
+      // the query's own point never enters its list
+      if (own >= base && own < base + nb) mark &= ~(1u << (own - base));
       __syncwarp();
       top.reserve(__popc(mark));
       while (mark) {

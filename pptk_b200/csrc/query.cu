@@ -30,13 +30,19 @@ TreeView<T, D> view_of(const TreeBase* t) {
   return v;
 }
 
-// Per-warp shared memory: leaf staging buffer (r-near), traversal stack, the
-// 32 x 33 distance matrix of the kNN bucket scan, and (normals) `logcap`
-// list slots per lane.
+// Per-warp shared memory: the staging buffer (a leaf chunk in r-near walks,
+// the warp's queries in kNN walks), traversal stack, the 32 x 33 distance
+// matrix of the kNN bucket scan, and (normals) `logcap` list slots per lane.
+template <typename T, int D>
+__host__ __device__ constexpr size_t stage_bytes() {
+  typedef typename DistOf<T>::type DistT;
+  return 32 * (sizeof(PointRec<T, D>) > sizeof(QStage<DistT, D>) ? sizeof(PointRec<T, D>) : sizeof(QStage<DistT, D>));
+}
+
 template <typename T, int D>
 __host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
-  return 32 * sizeof(PointRec<T, D>) + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
+  return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
          ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + (size_t)logcap * 32 * 4;
 }
 
@@ -48,7 +54,7 @@ __device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap 
   unsigned char* base = qsm + (threadIdx.x >> 5) * per;
   WarpScratch<T, D> ws;
   ws.buf = (PointRec<T, D>*)base;
-  base += 32 * sizeof(PointRec<T, D>);
+  base += stage_bytes<T, D>();
   ws.stack = (int*)base;
   base += ((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15;
   ws.dmat = (DistT*)base;
