@@ -48,6 +48,9 @@ extern std::atomic<long long> g_launches;
 //  lane_span: a kNN warp whose queries span more than this many tree
 //    positions walks the tree per lane instead of as a packet (-1: never).
 extern std::atomic<int> g_tune_lane_span;
+//  rnear_warp_queries: r-near batches of at most this many queries run one
+//    warp per query instead of 32-query packets (0: never).
+extern std::atomic<int> g_tune_rnear_warp_queries;
 
 // Status sink of this host thread (pptkg_set_status_sink): while set, query
 // entry points record kernel check failures into this device word and

@@ -12,6 +12,7 @@ namespace pptkg {
 
 std::atomic<long long> g_launches{0};
 std::atomic<int> g_tune_lane_span{256};
+std::atomic<int> g_tune_rnear_warp_queries{262144};
 thread_local int* g_status_sink = nullptr;
 
 namespace {
@@ -93,6 +94,11 @@ int pptkg_tune_set(const char* name, int64_t value) {
     pptkg::g_tune_lane_span.store((int)value);
     return PPTKG_OK;
   }
+  if (std::string(name) == "rnear_warp_queries") {
+    if (value < 0 || value > INT32_MAX) return PPTKG_E_INVALID;
+    pptkg::g_tune_rnear_warp_queries.store((int)value);
+    return PPTKG_OK;
+  }
   return PPTKG_E_INVALID;
 }
 
@@ -105,6 +111,10 @@ int pptkg_tune_get(const char* name, int64_t* value) {
   if (!name || !value) return PPTKG_E_INVALID;
   if (std::string(name) == "lane_span") {
     *value = pptkg::g_tune_lane_span.load();
+    return PPTKG_OK;
+  }
+  if (std::string(name) == "rnear_warp_queries") {
+    *value = pptkg::g_tune_rnear_warp_queries.load();
     return PPTKG_OK;
   }
   return PPTKG_E_INVALID;

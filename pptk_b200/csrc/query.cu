@@ -637,6 +637,174 @@ __global__ void __launch_bounds__(QTHREADS) k_rnear_fill(TreeView<T, D> tv, L ld
   if (overflow || w != wend) atomicExch(status, 2);
 }
 
+// r-near with one warp per query, for batches too small to fill the GPU as
+// 32-query packets (a packet lane walks its own hits one by one, so a few
+// thousand queries with 1e4-1e5 hits each leave most of the GPU idle).  The
+// warp walks its query's path once, with all lanes in step: lane j tests
+// tree position base + j of each bucket chunk, and a child box inside the
+// ball is taken whole, its positions [begin, begin + cnt) in strided passes.
+// Children are visited left before right and hits written by ballot rank,
+// so they come out in ascending tree position: the same set and order as
+// the packet walk (kdtree-impl.h:519-558).  Subtree start positions are
+// carried down the walk (a left child starts where its parent does, a right
+// child cnt[0] later) and checked against every leaf reached.
+// COUNT: counts[qid] = hits, the query's own point excluded as in
+// k_rnear_count; otherwise out[off[qid] ...] = original indices of the hits.
+template <typename T, int D, typename L, bool COUNT>
+__global__ void __launch_bounds__(QTHREADS) k_rnear_warp(TreeView<T, D> tv, L ld, const int* order, int order_mode,
+                                                         int m, typename DistOf<T>::type r2, int stack_ints,
+                                                         int64_t* counts, const int64_t* off, int32_t* out,
+                                                         int* status) {
+  typedef typename DistOf<T>::type DistT;
+  extern __shared__ __align__(16) int rw_stack[];
+  const int w = blockIdx.x * QWARPS + (threadIdx.x >> 5);
+  if (w >= m) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lt = (1u << lane) - 1u;
+  int* stk = rw_stack + (threadIdx.x >> 5) * stack_ints;
+  const int qid = query_of(w, order, order_mode, tv);
+  DistT q[D];
+  int own = -1;
+  const bool active = ld.load(qid, tv, q, own);
+  long long cnt = 0;
+  int64_t wp = 0, wend = 0;
+  if (!COUNT && active) {
+    wp = off[qid];
+    wend = off[qid + 1];
+  }
+  bool bad = false;
+  // positions [begin, begin + n): every one a hit (whole) or tested
+  auto run = [&](int begin, int n, bool whole) {
+    for (int base = begin; base < begin + n; base += 32) {
+      const int p = base + lane;
+      bool hit = false;
+      int32_t id = 0;
+      if (p < begin + n) {
+        if (whole) {
+          hit = COUNT || p != own;
+          if (!COUNT && hit) id = tv.pts[p].id;
+        } else {
+          const PointRec<T, D> pr = tv.pts[p];
+          hit = point_dist2<T, DistT, D>(pr.c, q) < r2 && (COUNT || p != own);
+          id = pr.id;
+        }
+      }
+      const unsigned hm = __ballot_sync(FULL, hit);
+      if (COUNT) {
+        cnt += __popc(hm);
+      } else {
+        if (hit) {
+          const int64_t at = wp + __popc(hm & lt);
+          if (at < wend)
+            out[at] = id;
+          else
+            bad = true;
+        }
+        wp += __popc(hm);
+      }
+    }
+    if (!COUNT) bad = __any_sync(FULL, bad);  // keep the walk's control flow warp-uniform
+  };
+  // child c of nd, whose positions start at cb: scans or takes it, or
+  // returns the inner node to descend into (-1: nothing to descend into)
+  auto take = [&](const TNode<T, D>& nd, int c, int cb) -> int {
+    const int n = nd.cnt[c];
+    if (n == 0 || !(box_min_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2)) return -1;
+    if (box_max_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2) {
+      if (COUNT)
+        cnt += n;
+      else
+        run(cb, n, true);
+      return -1;
+    }
+    if (nd.ref[c] < 0) {
+      if (-nd.ref[c] - 1 != cb) {
+        bad = true;
+        return -1;
+      }
+      run(cb, n, false);
+      return -1;
+    }
+    return nd.ref[c];
+  };
+  if (active) {
+    int sp = 0, cur = tv.root, b = 0, visits = 0;
+    while (!bad) {
+      if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
+        bad = true;
+        break;
+      }
+      const TNode<T, D> nd = load_node(tv.nodes, cur);
+      const int b1 = b + nd.cnt[0];
+      int next = take(nd, 0, b);
+      if (next >= 0) {
+        // into the left subtree; the right child waits if the ball reaches it
+        if (nd.cnt[1] > 0 && box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) < r2) {
+          if (2 * sp + 2 > stack_ints) {
+            bad = true;
+            break;
+          }
+          __syncwarp();
+          if (lane == 0) {
+            stk[2 * sp] = cur * 2 + 1;
+            stk[2 * sp + 1] = b1;
+          }
+          __syncwarp();
+          sp++;
+        }
+        cur = next;
+        continue;
+      }
+      next = take(nd, 1, b1);
+      if (next >= 0) {
+        cur = next;
+        b = b1;
+        continue;
+      }
+      bool found = false;
+      while (sp > 0 && !bad) {
+        --sp;
+        const int e = stk[2 * sp], eb = stk[2 * sp + 1];
+        const int r = take(load_node(tv.nodes, e >> 1), e & 1, eb);
+        if (r >= 0) {
+          cur = r;
+          b = eb;
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+  }
+  bad = __any_sync(FULL, bad);
+  if (lane != 0) return;
+  if (COUNT) {
+    if (own >= 0 && cnt > 0) cnt -= 1;  // the point itself is always a hit when r2 > 0
+    counts[qid] = active ? cnt : 0;
+    if (bad) atomicExch(status, 1);
+  } else if (bad || wp != wend) {
+    atomicExch(status, 2);
+  }
+}
+
+// Per-warp stack of k_rnear_warp: (child ref, start position) pairs, one per
+// level at most.
+inline int rnear_warp_stack_ints(int depth) { return (2 * (depth + 1) + 3) & ~3; }
+
+template <typename T, int D, typename L, bool COUNT>
+void launch_rnear_warp(const TreeBase* t, L ld, const int* order, int mode, int m, typename DistOf<T>::type r2,
+                       int64_t* counts, const int64_t* off, int32_t* out, int* status, cudaStream_t st) {
+  const int si = rnear_warp_stack_ints(t->tdepth);
+  const size_t smem = (size_t)QWARPS * si * sizeof(int);
+  if (smem > 48 * 1024)
+    PPTKG_CUDA(cudaFuncSetAttribute(k_rnear_warp<T, D, L, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  k_rnear_warp<T, D, L, COUNT><<<div_up(m, QWARPS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, r2,
+                                                                            si, counts, off, out, status);
+  PPTKG_CHECK_LAUNCH();
+}
+
 template <typename T, int D, typename F>
 void with_loader(const TreeBase* t, const QuerySpec& qs, F&& f) {
   if (qs.pts) {
@@ -668,6 +836,10 @@ int64_t rnear_count(const TreeBase* t, const QuerySpec& qs, double dmax, int64_t
   Stage stage("rnear_count", st);
   with_loader<T, D>(t, qs, [&](auto ld) {
     typedef decltype(ld) L;
+    if (m <= g_tune_rnear_warp_queries.load()) {
+      launch_rnear_warp<T, D, L, true>(t, ld, order.get(), mode, m, r2, d_off, nullptr, nullptr, status.get(), st);
+      return;
+    }
     if (smem > 48 * 1024)
       PPTKG_CUDA(cudaFuncSetAttribute(k_rnear_count<T, D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_rnear_count<T, D, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order.get(), mode, m,
@@ -697,6 +869,10 @@ void rnear_fill(const TreeBase* t, const QuerySpec& qs, double dmax, const int64
   Stage stage("rnear_fill", st);
   with_loader<T, D>(t, qs, [&](auto ld) {
     typedef decltype(ld) L;
+    if (m <= g_tune_rnear_warp_queries.load()) {
+      launch_rnear_warp<T, D, L, false>(t, ld, order.get(), mode, m, r2, nullptr, d_off, d_out, status.get(), st);
+      return;
+    }
     if (smem > 48 * 1024)
       PPTKG_CUDA(cudaFuncSetAttribute(k_rnear_fill<T, D, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_rnear_fill<T, D, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order.get(), mode, m, r2,

@@ -115,6 +115,44 @@ def test_rnear_matches_oracle_and_brute_force(gpu, port):
     assert np.array_equal(off, ooff) and np.array_equal(out, oout)
 
 
+@pytest.mark.parametrize("dtype,dim", [(np.float32, 3), (np.float64, 3), (np.float32, 2), (np.float64, 4),
+                                       (np.int16, 3)])
+def test_rnear_warp_per_query_matches_packets_and_oracle(gpu, port, dtype, dim):
+    # small batches give each query a whole warp (rnear_warp_queries); both
+    # forms must return the oracle's hits in its order, for point and self
+    # queries, radii from a few hits to most of the cloud (whole boxes taken
+    # without distance tests) and the all-points form
+    from pptk_b200 import _native as N
+    rng = np.random.default_rng(21 + dim)
+    scale = 1000.0 if np.issubdtype(dtype, np.integer) else 1.0
+    P = (rng.random((40_000, dim)) * scale).astype(dtype)
+    P[::997] = P[1::997]
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    q = (rng.random((1000, dim)) * scale).astype(np.float32 if np.issubdtype(dtype, np.integer) else dtype)
+    sidx = np.arange(0, len(P), 41, dtype=np.int32)
+    default = N.tune_get("rnear_warp_queries")
+    try:
+        for r in (0.03 * scale, 0.2 * scale, 0.6 * scale):
+            rr = float(np.float32(r))
+            ooff, oout = o.rnear(q, rr)
+            soff, sout = o.rnear_self(sidx, rr)
+            for wq in (0, 1 << 30):
+                N.tune_set("rnear_warp_queries", wq)
+                off, out = gpu.kdtree.rnear(t, q, r)
+                assert np.array_equal(off, ooff) and np.array_equal(out, oout), (r, wq)
+                off, out = gpu.kdtree.rnear(t, sidx, r)
+                assert np.array_equal(off, soff) and np.array_equal(out, sout), (r, wq)
+        r = 0.01 * scale
+        aoff, aout = o.rnear_self(np.arange(len(P), dtype=np.int32), float(np.float32(r)))
+        for wq in (0, 1 << 30):
+            N.tune_set("rnear_warp_queries", wq)
+            off, out = gpu.kdtree.rnear(t, None, r)
+            assert np.array_equal(off, aoff) and np.array_equal(out, aout), wq
+    finally:
+        N.tune_set("rnear_warp_queries", default)
+
+
 def test_edge_cases(gpu, port):
     kd = gpu.kdtree
     # empty input
