@@ -283,7 +283,7 @@ def device_timed(ctx, fn, steps):
 # tree-order queries (profiles/k_normals_plain_lidar8M.md) and scattered
 # serving queries (profiles/k_normals_k_knn_serving_lidar8M.md); the bench's
 # per-launch traffic is this figure times the queries of a launch.
-TRAFFIC_PER_QUERY = {"tree_order": 111.8, "scattered": 160.5}
+TRAFFIC_PER_QUERY = {"tree_order": 126.8, "scattered": 160.5}
 
 
 def roofline(ctx, stage_name, queries, traffic_kind):
