@@ -384,9 +384,9 @@ def run_ragged_workload(args, ctx):
     ctx.lib.pptkg_profile_enable(1)
     ms, launches, clk = device_timed(ctx, step, args.steps)
     stages = {}
-    for nm in ("build", "build.levels", "build.subtree", "forest.knn", "forest.normals"):
+    for nm in BUILD_STAGES[:7] + ("forest.knn", "forest.normals"):
         t_, c_ = ctx.stage(nm)
-        stages[nm] = t_ / max(c_, 1) if c_ else 0.0
+        stages[nm] = {"ms_per_step": t_ / args.steps, "calls_per_step": c_ / args.steps}
     roof = roofline(ctx, "forest.normals", n * args.steps, "tree_order")
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)

@@ -1021,8 +1021,10 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   const int small_cap = small_capacity<T, D>(max_leaf, cap_list, smem);
   // a binary tree over nv points has at most 2 nv - 1 records
   const size_t rec_cap = 2 * (size_t)nv + 64;
+  std::unique_ptr<Stage> st_scr(new Stage("build.scratch", st));
   DevBuf<Rec<T, D>> recbuf(rec_cap, st);
   Rec<T, D>* recs = recbuf.get();
+  st_scr.reset();
 
   // large segments per level are disjoint and above small_cap points
   const int seg_cap = nv / (small_cap + 1) + 2;
@@ -1118,10 +1120,12 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   }
   if ((size_t)tree->n_recs > rec_cap) throw Error(E_DEVICE, "device build: record capacity exceeded");
   tree->depth = depth;
+  std::unique_ptr<Stage> st_rec(new Stage("build.records", st));
   PPTKG_CUDA(cudaMallocAsync(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>), st));
   if (tree->n_recs)
     PPTKG_CUDA(cudaMemcpyAsync(tree->recs, recs, tree->n_recs * sizeof(Rec<T, D>), cudaMemcpyDeviceToDevice, st));
   recbuf.release();
+  st_rec.reset();
 
   // tree-ordered points and the forward map
   std::unique_ptr<Stage> st_fin(new Stage("build.finish", st));
@@ -1142,6 +1146,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
     make_tnodes<T, D>(tree.get(), bucket, st);
   }
 
+  Stage st_root("build.root", st);
   Rec<T, D> r0;
   int root0 = -1;
   PPTKG_CUDA(cudaMemcpyAsync(&root0, tree->root_rec, sizeof(int), cudaMemcpyDeviceToHost, st));
