@@ -69,6 +69,8 @@ def parse():
     p.add_argument("--k", type=int, default=16)
     p.add_argument("--slots", type=int, default=3)
     p.add_argument("--max-batch", type=int, default=20_000_000, help="queries folded into one server batch")
+    p.add_argument("--max-host-batch", type=int, default=8_000_000,
+                   help="queries folded into one server batch that returns numpy results")
     p.add_argument("--plain-sample", type=int, default=24, help="requests timed through the plain calls")
     p.add_argument("--latency-seconds", type=float, default=3.0)
     p.add_argument("--cpu-sample", type=int, default=1_000_000)
@@ -686,7 +688,8 @@ def run_serving_workload(args, ctx):
         return out
 
     warm_dev, mix_dev = device_requests(warm_mix), device_requests(mix)
-    srv = serving.Server(budget_bytes=150e9, slots=args.slots, max_batch_queries=args.max_batch)
+    srv = serving.Server(budget_bytes=150e9, slots=args.slots, max_batch_queries=args.max_batch,
+                         max_host_batch_queries=args.max_host_batch)
     tid = srv.build(dev).result()
 
     def submit(reqs):

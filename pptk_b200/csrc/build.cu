@@ -931,13 +931,13 @@ __global__ void k_lower_tnodes(const TNode<T, D>* in, int n, TNode<float, D>* ou
 template <typename T, int D>
 void lower_points(TreeBase* tree, cudaStream_t st) {
   PointRec<float, D>* out = nullptr;
-  PPTKG_CUDA(cudaMallocAsync((void**)&out, std::max<int64_t>(tree->nv, 1) * sizeof(PointRec<float, D>), st));
+  PPTKG_CUDA(dev_malloc((void**)&out, std::max<int64_t>(tree->nv, 1) * sizeof(PointRec<float, D>), st));
   if (tree->nv > 0) {
     k_lower_points<T, D><<<(unsigned)((tree->nv + 255) / 256), 256, 0, st>>>((const PointRec<T, D>*)tree->pts,
                                                                              tree->nv, out);
     PPTKG_CHECK_LAUNCH();
   }
-  PPTKG_CUDA(cudaFreeAsync(tree->pts, st));
+  dev_free(tree->pts, st);
   tree->pts = out;
   tree->dtype = F32;
 }
@@ -946,12 +946,12 @@ template <typename T, int D>
 void lower_tnodes(TreeBase* tree, cudaStream_t st) {
   TNode<float, D>* out = nullptr;
   const int n = tree->n_tnodes;
-  PPTKG_CUDA(cudaMallocAsync((void**)&out, std::max(n, 1) * sizeof(TNode<float, D>), st));
+  PPTKG_CUDA(dev_malloc((void**)&out, std::max(n, 1) * sizeof(TNode<float, D>), st));
   if (n > 0) {
     k_lower_tnodes<T, D><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const TNode<T, D>*)tree->tnodes, n, out);
     PPTKG_CHECK_LAUNCH();
   }
-  PPTKG_CUDA(cudaFreeAsync(tree->tnodes, st));
+  dev_free(tree->tnodes, st);
   tree->tnodes = out;
 }
 
@@ -979,16 +979,16 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
     throw Error(E_INVALID, "cloud offsets must start at 0 and end at n");
   for (int c = 0; c < ncloud; c++)
     if (tree->orig_off_h[c + 1] < tree->orig_off_h[c]) throw Error(E_INVALID, "cloud offsets must not decrease");
-  PPTKG_CUDA(cudaMallocAsync((void**)&tree->orig_off, sizeof(int64_t) * (ncloud + 1), st));
-  PPTKG_CUDA(cudaMallocAsync((void**)&tree->valid_off, sizeof(int64_t) * (ncloud + 1), st));
-  PPTKG_CUDA(cudaMallocAsync((void**)&tree->root_rec, sizeof(int) * ncloud, st));
-  PPTKG_CUDA(cudaMallocAsync((void**)&tree->root_tnode, sizeof(int) * ncloud, st));
+  PPTKG_CUDA(dev_malloc((void**)&tree->orig_off, sizeof(int64_t) * (ncloud + 1), st));
+  PPTKG_CUDA(dev_malloc((void**)&tree->valid_off, sizeof(int64_t) * (ncloud + 1), st));
+  PPTKG_CUDA(dev_malloc((void**)&tree->root_rec, sizeof(int) * ncloud, st));
+  PPTKG_CUDA(dev_malloc((void**)&tree->root_tnode, sizeof(int) * ncloud, st));
   PPTKG_CUDA(cudaMemcpyAsync(tree->orig_off, orig_off_h, sizeof(int64_t) * (ncloud + 1), cudaMemcpyHostToDevice, st));
   PPTKG_CUDA(cudaMemsetAsync(tree->root_rec, 0xff, sizeof(int) * ncloud, st));
 
   // valid-point compaction (ValidPointIndices, kdtree-impl.h:53-75), per cloud
   std::unique_ptr<Stage> st_prep(new Stage("build.prep", st));
-  DevBuf<int> flag(n + 1, st), off(n + 1, st);
+  BuildBuf<int> flag(n + 1, st), off(n + 1, st);
   if (n > 0) {
     k_valid<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get());
     PPTKG_CHECK_LAUNCH();
@@ -1003,8 +1003,8 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   const int nv = (int)tree->valid_off_h[ncloud];
   tree->nv = nv;
 
-  DevBuf<T> xs((size_t)D * nv + 1, st);
-  DevBuf<int> ids(nv + 1, st);
+  BuildBuf<T> xs((size_t)D * nv + 1, st);
+  BuildBuf<int> ids(nv + 1, st);
   SoA<T, D> soa;
   for (int d = 0; d < D; d++) soa.x[d] = xs.get() + (size_t)d * nv;
   soa.id = ids.get();
@@ -1022,7 +1022,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   // a binary tree over nv points has at most 2 nv - 1 records
   const size_t rec_cap = 2 * (size_t)nv + 64;
   std::unique_ptr<Stage> st_scr(new Stage("build.scratch", st));
-  DevBuf<Rec<T, D>> recbuf(rec_cap, st);
+  BuildBuf<Rec<T, D>> recbuf(rec_cap, st);
   Rec<T, D>* recs = recbuf.get();
   st_scr.reset();
 
@@ -1033,10 +1033,10 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   int depth = 0;
   for (int attempt = 0; attempt < 4; attempt++, small_capn *= 4) {
     Stage st_att("build.attempt", st);
-    DevBuf<BuildCtl> ctl(1, st);
+    BuildBuf<BuildCtl> ctl(1, st);
     PPTKG_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(BuildCtl), st));
-    DevBuf<Seg<T, D>> segL[2] = {DevBuf<Seg<T, D>>(seg_cap, st), DevBuf<Seg<T, D>>(seg_cap, st)};
-    DevBuf<Seg<T, D>> smallL(small_capn, st);
+    BuildBuf<Seg<T, D>> segL[2] = {BuildBuf<Seg<T, D>>(seg_cap, st), BuildBuf<Seg<T, D>>(seg_cap, st)};
+    BuildBuf<Seg<T, D>> smallL(small_capn, st);
     if (nv > 0) {
       k_roots<T, D><<<div_up(ncloud, 128), 128, 0, st>>>(tree->valid_off, tree->orig_off, ncloud, small_cap,
                                                           segL[0].get(), smallL.get(), small_capn, ctl.get());
@@ -1045,9 +1045,9 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
     int levels = 0;
     {
       Stage st_levels("build.levels", st);
-      DevBuf<int> blpos(nv + 1, st), grpos(nv + 1, st);
-      DevBuf<int> tile_seg(max_tiles, st);
-      DevBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
+      BuildBuf<int> blpos(nv + 1, st), grpos(nv + 1, st);
+      BuildBuf<int> tile_seg(max_tiles, st);
+      BuildBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
       const unsigned gt = (unsigned)max_tiles;
       const unsigned gs = (unsigned)div_up(seg_cap, 128);
       int h0 = 0;
@@ -1121,7 +1121,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   if ((size_t)tree->n_recs > rec_cap) throw Error(E_DEVICE, "device build: record capacity exceeded");
   tree->depth = depth;
   std::unique_ptr<Stage> st_rec(new Stage("build.records", st));
-  PPTKG_CUDA(cudaMallocAsync(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>), st));
+  PPTKG_CUDA(dev_malloc(&tree->recs, std::max(tree->n_recs, 1) * sizeof(Rec<T, D>), st));
   if (tree->n_recs)
     PPTKG_CUDA(cudaMemcpyAsync(tree->recs, recs, tree->n_recs * sizeof(Rec<T, D>), cudaMemcpyDeviceToDevice, st));
   recbuf.release();
@@ -1130,9 +1130,9 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
   // tree-ordered points and the forward map
   std::unique_ptr<Stage> st_fin(new Stage("build.finish", st));
   PointRec<T, D>* pts = nullptr;
-  PPTKG_CUDA(cudaMallocAsync((void**)&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>), st));
+  PPTKG_CUDA(dev_malloc((void**)&pts, std::max<int64_t>(nv, 1) * sizeof(PointRec<T, D>), st));
   tree->pts = pts;
-  PPTKG_CUDA(cudaMallocAsync((void**)&tree->fwd, std::max<int64_t>(n, 1) * sizeof(int), st));
+  PPTKG_CUDA(dev_malloc((void**)&tree->fwd, std::max<int64_t>(n, 1) * sizeof(int), st));
   if (n > 0) PPTKG_CUDA(cudaMemsetAsync(tree->fwd, 0xff, n * sizeof(int), st));
   if (nv > 0) {
     k_finish<T, D><<<div_up(nv, 256), 256, 0, st>>>(soa, nv, pts, tree->fwd);
@@ -1172,14 +1172,14 @@ TreeBase* build_tree(const T* d_in, int64_t n, int max_leaf, double thr, int buc
 template <typename T, int D>
 void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
   if (tree->tnodes) {
-    PPTKG_CUDA(cudaFreeAsync(tree->tnodes, st));
+    dev_free(tree->tnodes, st);
     tree->tnodes = nullptr;
   }
   if (bucket < 1) bucket = 1;
   tree->bucket = bucket;
   const int nr = tree->n_recs;
   const Rec<T, D>* recs = (const Rec<T, D>*)tree->recs;
-  DevBuf<int> flag(nr + 1, st), tid(nr + 1, st);
+  BuildBuf<int> flag(nr + 1, st), tid(nr + 1, st);
   int nt = 0;
   if (nr > 0) {
     k_tflag<T, D><<<div_up(nr, 256), 256, 0, st>>>(recs, nr, bucket, flag.get());
@@ -1189,7 +1189,7 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
     PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   TNode<T, D>* nodes = nullptr;
-  PPTKG_CUDA(cudaMallocAsync((void**)&nodes, (size_t)(nt + tree->ncloud) * sizeof(TNode<T, D>), st));
+  PPTKG_CUDA(dev_malloc((void**)&nodes, (size_t)(nt + tree->ncloud) * sizeof(TNode<T, D>), st));
   tree->tnodes = nodes;
   tree->n_tnodes = nt + tree->ncloud;
   if (nt > 0) {
@@ -1217,16 +1217,16 @@ size_t TreeBase::device_bytes() const {
 
 TreeBase::~TreeBase() {
   // stream-ordered release on the stream the tree was built on
-  if (pts) cudaFreeAsync(pts, stream);
-  if (recs) cudaFreeAsync(recs, stream);
-  if (tnodes) cudaFreeAsync(tnodes, stream);
-  if (fwd) cudaFreeAsync(fwd, stream);
-  if (root_rec) cudaFreeAsync(root_rec, stream);
-  if (root_tnode) cudaFreeAsync(root_tnode, stream);
-  if (valid_off) cudaFreeAsync(valid_off, stream);
-  if (orig_off) cudaFreeAsync(orig_off, stream);
-  if (slot_off) cudaFreeAsync(slot_off, stream);
-  if (warp_cloud) cudaFreeAsync(warp_cloud, stream);
+  if (pts) dev_free(pts, stream);
+  if (recs) dev_free(recs, stream);
+  if (tnodes) dev_free(tnodes, stream);
+  if (fwd) dev_free(fwd, stream);
+  if (root_rec) dev_free(root_rec, stream);
+  if (root_tnode) dev_free(root_tnode, stream);
+  if (valid_off) dev_free(valid_off, stream);
+  if (orig_off) dev_free(orig_off, stream);
+  if (slot_off) dev_free(slot_off, stream);
+  if (warp_cloud) dev_free(warp_cloud, stream);
 }
 
 #endif  // PPTKG_BUILD_INT

@@ -278,11 +278,11 @@ TreeBase* load_tree(const char* buf, size_t size, cudaStream_t st) {
   void** dst[8] = {&t->pts, (void**)&t->fwd, &t->recs, &t->tnodes, (void**)&t->root_rec, (void**)&t->root_tnode,
                    (void**)&t->valid_off, (void**)&t->orig_off};
   for (int s = 0; s < 8; s++) {
-    PPTKG_CUDA(cudaMallocAsync(dst[s], std::max<size_t>((size_t)want[s], 1), st));
+    PPTKG_CUDA(dev_malloc(dst[s], std::max<size_t>((size_t)want[s], 1), st));
     if (want[s]) PPTKG_CUDA(cudaMemcpyAsync(*dst[s], buf + off[s], (size_t)want[s], cudaMemcpyHostToDevice, st));
   }
   // device checks of every reference a query follows
-  DevBuf<int> bad(1, st);
+  BuildBuf<int> bad(1, st);
   PPTKG_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(int), st));
   with_types(h.dtype, h.rec_dtype, h.dim, [&](auto tq, auto tr, auto d) {
     typedef decltype(tq) Tq;

@@ -1362,10 +1362,10 @@ static SlotMap slot_map(const TreeBase* t, int64_t& n_slots, cudaStream_t st) {
     }
     mt->n_slots = so[t->ncloud];
     if (mt->n_slots > INT32_MAX) throw Error(E_INVALID, "forest too large for one query pass");
-    PPTKG_CUDA(cudaMallocAsync((void**)&mt->slot_off, sizeof(int64_t) * (t->ncloud + 1), st));
+    PPTKG_CUDA(dev_malloc((void**)&mt->slot_off, sizeof(int64_t) * (t->ncloud + 1), st));
     PPTKG_CUDA(cudaMemcpyAsync(mt->slot_off, so.data(), sizeof(int64_t) * (t->ncloud + 1), cudaMemcpyHostToDevice, st));
     const int64_t nw = std::max<int64_t>(mt->n_slots / 32, 1);
-    PPTKG_CUDA(cudaMallocAsync((void**)&mt->warp_cloud, sizeof(int) * nw, st));
+    PPTKG_CUDA(dev_malloc((void**)&mt->warp_cloud, sizeof(int) * nw, st));
     if (mt->n_slots > 0) {
       k_warp_cloud<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(mt->slot_off, t->ncloud, nw, mt->warp_cloud);
       PPTKG_CHECK_LAUNCH();

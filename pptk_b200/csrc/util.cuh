@@ -11,10 +11,28 @@ namespace pptkg {
 // threshold is 0), so repeated calls reuse their scratch without remapping.
 void keep_pool_cached(cudaStream_t st);
 
+// Device memory of trees and of the build path.  Freed blocks of 1 MB and
+// more are kept in a cache per (device, stream); smaller ones go back to the
+// pool.  An allocation takes a block freed on its own stream
+// (stream order makes that safe without any synchronisation), else one freed
+// on another stream of the device whose free event (recorded on that stream
+// at the free) has completed; misses come from the stream-ordered pool.  On
+// a stream that is capturing a CUDA graph both calls go straight to
+// cudaMallocAsync / cudaFreeAsync, so captured work keeps graph-owned memory.  The cache exists because cudaMallocAsync, even on
+// memory the pool already holds, was measured to stall the calling thread for
+// 0.1-1.7 s at times on 1-15 GB requests, leaving the GPU idle.  A request
+// that the pool cannot meet empties the cache of every stream of the device
+// and is tried once more.  dev_free takes the stream whose order protects
+// the block's last use (the stream it was used on).
+cudaError_t dev_malloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+
 // ------------------------------------------------------------- DevBuf ----
-// Scratch memory from the device's stream-ordered pool (cudaMallocAsync); it
-// is returned to the pool on the same stream when the buffer goes away.
-template <typename T>
+// Scratch memory that goes back when the buffer goes away, on the stream it
+// was allocated for: from the stream-ordered pool, or (CACHED) from
+// dev_malloc.  The build path uses the cached form: its scratch is large
+// (up to 2 records per point) and allocated on one stream per build.
+template <typename T, bool CACHED = false>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
@@ -25,10 +43,20 @@ struct DevBuf {
     release();
     s = stream;
     n = count;
-    if (count) PPTKG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
+    if (count) {
+      if (CACHED)
+        PPTKG_CUDA(dev_malloc((void**)&p, count * sizeof(T), stream));
+      else
+        PPTKG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
+    }
   }
   void release() {
-    if (p) cudaFreeAsync(p, s);
+    if (p) {
+      if (CACHED)
+        dev_free(p, s);
+      else
+        cudaFreeAsync(p, s);
+    }
     p = nullptr;
     n = 0;
   }
@@ -37,6 +65,10 @@ struct DevBuf {
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
 };
+
+// Scratch of the build path.
+template <typename T>
+using BuildBuf = DevBuf<T, true>;
 
 // ------------------------------------------------------ block primitives --
 template <typename V>
