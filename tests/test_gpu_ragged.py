@@ -107,6 +107,30 @@ def test_captured_forest_queries_replay(gpu):
     assert torch.equal(torch.nan_to_num(ev, nan=-9.0), torch.nan_to_num(ref_n, nan=-9.0))
 
 
+def test_builds_on_alternating_streams_agree(gpu):
+    # forest builds take their scratch and tree arrays from a per-stream
+    # cache of freed device blocks, reused across streams once idle; builds
+    # and frees alternating between two streams must give identical forests
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=12, count=60)
+    dev = torch.from_numpy(P).cuda()
+    base_i, base_c = ragged.Forest(dev, off).knn(6)
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    keep = []
+    for i in range(6):
+        s = streams[i % 2]
+        with torch.cuda.stream(s):
+            f = ragged.Forest(dev, off)
+            idx, cnt = f.knn(6)
+        s.synchronize()
+        assert torch.equal(idx, base_i) and torch.equal(cnt, base_c), i
+        keep.append(f)
+        if len(keep) > 1:
+            keep.pop(0)  # frees the forest built on the other stream
+
+
 def test_capture_needs_device_forest(gpu):
     from pptk_b200 import ragged
     P, off, _ = small_batch(seed=5, count=12)
