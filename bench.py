@@ -550,7 +550,7 @@ def run_multitree_workload(args, ctx):
         pending = []
         for rq in stream_reqs:
             while time.perf_counter() < nxt:
-                time.sleep(min(nxt - time.perf_counter(), 0.002))
+                time.sleep(max(0.0, min(nxt - time.perf_counter(), 0.002)))
             pending.append((rq, submit(rq)))
             nxt += arr.exponential(1.0 / rate)
             if time.perf_counter() - t_start > args.latency_seconds:
