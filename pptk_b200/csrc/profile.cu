@@ -193,90 +193,6 @@ void dev_free(void* p, cudaStream_t st) {
   g_live.erase(it);
 }
 
-// ------------------------------------------------------- query arenas --
-namespace {
-struct Arena {
-  char* base = nullptr;
-  size_t cap = 0;     // bytes of the arena
-  size_t off = 0;     // next free byte
-  size_t demand = 0;  // bytes asked for since the last start-over
-  long live = 0;      // blocks of this round not yet released (arena or pool)
-};
-typedef std::pair<int, cudaStream_t> ArenaKey;
-std::mutex g_armu;
-std::map<ArenaKey, Arena> g_arenas;
-std::unordered_map<void*, ArenaKey> g_overflow;  // pool blocks handed out while an arena was short
-
-// One block of the round released (g_armu held): once none is left the
-// arena starts over, reallocated first if the round asked for more.
-void arena_release_one(Arena& a, cudaStream_t st) {
-  if (--a.live > 0) return;
-  a.live = 0;
-  a.off = 0;
-  if (a.demand > a.cap) {
-    const size_t q = (size_t)2 << 20;
-    const size_t want = (a.demand + a.demand / 4 + q - 1) / q * q;
-    if (a.base) cudaFreeAsync(a.base, st);
-    a.base = nullptr;
-    a.cap = 0;
-    void* nb = nullptr;
-    if (cudaMallocAsync(&nb, want, st) == cudaSuccess) {
-      a.base = (char*)nb;
-      a.cap = want;
-    } else {
-      cudaGetLastError();  // the next round takes its blocks from the pool
-    }
-  }
-  a.demand = 0;
-}
-}  // namespace
-
-cudaError_t arena_malloc(void** p, size_t bytes, cudaStream_t st) {
-  *p = nullptr;
-  if (capturing(st)) return cudaMallocAsync(p, bytes ? bytes : 1, st);
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  const size_t need = ((bytes ? bytes : 1) + 255) / 256 * 256;
-  std::lock_guard<std::mutex> g(g_armu);
-  const ArenaKey key{dev, st};
-  Arena& a = g_arenas[key];
-  if (a.off + need <= a.cap) {
-    *p = a.base + a.off;
-    a.off += need;
-  } else {
-    e = cudaMallocAsync(p, need, st);
-    if (e != cudaSuccess) {
-      *p = nullptr;
-      return e;
-    }
-    g_overflow[*p] = key;
-  }
-  a.demand += need;
-  a.live++;
-  return cudaSuccess;
-}
-
-void arena_free(void* p, cudaStream_t st) {
-  if (!p) return;
-  std::lock_guard<std::mutex> g(g_armu);
-  auto o = g_overflow.find(p);
-  if (o != g_overflow.end()) {
-    const ArenaKey key = o->second;
-    g_overflow.erase(o);
-    cudaFreeAsync(p, st);
-    arena_release_one(g_arenas[key], key.second);
-    return;
-  }
-  for (auto& kv : g_arenas) {
-    Arena& a = kv.second;
-    if (kv.first.second != st || !a.base || (char*)p < a.base || (char*)p >= a.base + a.cap) continue;
-    arena_release_one(a, st);
-    return;
-  }
-  cudaFreeAsync(p, st);  // allocated while the stream was capturing
-}
-
 void keep_pool_cached(cudaStream_t) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;

@@ -27,19 +27,9 @@ void keep_pool_cached(cudaStream_t st);
 cudaError_t dev_malloc(void** p, size_t bytes, cudaStream_t st);
 void dev_free(void* p, cudaStream_t st);
 
-// Query scratch.  Each (device, stream) has one arena, handed out bump-wise;
-// when every block of it has been released the arena starts over, and if
-// that round asked for more than it holds it is reallocated at that size
-// first (the excess came from the pool meanwhile).  Stream order makes the
-// reuse safe: the kernels of earlier calls on the stream come first.  After
-// the first calls of a given size the query path makes no pool calls.  A
-// stream capturing a CUDA graph goes straight to the pool.
-cudaError_t arena_malloc(void** p, size_t bytes, cudaStream_t st);
-void arena_free(void* p, cudaStream_t st);
-
 // ------------------------------------------------------------- DevBuf ----
 // Scratch memory that goes back when the buffer goes away, on the stream it
-// was allocated for: from the stream's query arena, or (CACHED) from
+// was allocated for: from the stream-ordered pool, or (CACHED) from
 // dev_malloc.  The build path uses the cached form: its scratch is large
 // (up to 2 records per point) and allocated on one stream per build.
 template <typename T, bool CACHED = false>
@@ -57,7 +47,7 @@ struct DevBuf {
       if (CACHED)
         PPTKG_CUDA(dev_malloc((void**)&p, count * sizeof(T), stream));
       else
-        PPTKG_CUDA(arena_malloc((void**)&p, count * sizeof(T), stream));
+        PPTKG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
     }
   }
   void release() {
@@ -65,7 +55,7 @@ struct DevBuf {
       if (CACHED)
         dev_free(p, s);
       else
-        arena_free(p, s);
+        cudaFreeAsync(p, s);
     }
     p = nullptr;
     n = 0;
