@@ -42,6 +42,25 @@ def test_c_abi_rejects_bad_arguments_without_a_gpu():
         N.check(N.E_INVALID, "x")
 
 
+def test_tuning_knobs_validate_and_round_trip():
+    # process-wide traversal knobs: defaults, accepted ranges, rejected values
+    from pptk_b200 import _native as N
+    lib = N.lib()
+    for name, default, good, bad in (("lane_span", 256, (-1, 0, 64, 1 << 20), (-2,)),
+                                     ("rnear_warp_queries", 262144, (0, 1, 1 << 30), (-1,))):
+        assert N.tune_get(name) == default
+        try:
+            for v in good:
+                N.tune_set(name, v)
+                assert N.tune_get(name) == v
+            for v in bad:
+                assert lib.pptkg_tune_set(name.encode(), ctypes.c_int64(v)) == N.E_INVALID
+                assert N.tune_get(name) == good[-1]
+        finally:
+            N.tune_set(name, default)
+    assert lib.pptkg_tune_set(b"no_such_knob", ctypes.c_int64(1)) == N.E_INVALID
+
+
 def test_index_extraction_follows_reference_rules():
     from pptk_b200._args import extract_indices
     assert extract_indices([0, -1, 3], 5).tolist() == [0, 4, 3]
