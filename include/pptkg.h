@@ -256,11 +256,13 @@ PPTKG_API int64_t pptkg_launch_count(void);
  *   "lane_span": a kNN / normals warp whose 32 queries span more than this
  *     many tree positions walks the tree per lane rather than as one packet
  *     (-1: always packets).  Default 256.
- *   "rnear_warp_queries": pptkg_rnear_count / pptkg_rnear_fill calls with
- *     at most this many queries give each query a whole warp (the lanes split
- *     every bucket) instead of packing 32 queries into a warp (0: never).
+ *   "rnear_warp_queries": pptkg_rnear_count / pptkg_rnear_fill calls, and
+ *     normals over r-near neighbourhoods (k = -1), with at most this many
+ *     queries give each query a whole warp (the lanes split every bucket)
+ *     instead of packing 32 queries into a warp (0: never).
  *     Default 262144 (below it, 32-query packets leave B200's 148 SMs short
- *     of warps).  Results do not depend on it.
+ *     of warps).  Hit lists and neighbourhood sizes do not depend on it;
+ *     normals agree to FP64 rounding (their sums add in another order).
  * Unknown names or out-of-range values: PPTKG_E_INVALID. */
 PPTKG_API int pptkg_tune_set(const char* name, int64_t value);
 PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);

@@ -637,17 +637,94 @@ __global__ void __launch_bounds__(QTHREADS) k_rnear_fill(TreeView<T, D> tv, L ld
   if (overflow || w != wend) atomicExch(status, 2);
 }
 
-// r-near with one warp per query, for batches too small to fill the GPU as
-// 32-query packets (a packet lane walks its own hits one by one, so a few
-// thousand queries with 1e4-1e5 hits each leave most of the GPU idle).  The
-// warp walks its query's path once, with all lanes in step: lane j tests
-// tree position base + j of each bucket chunk, and a child box inside the
-// ball is taken whole, its positions [begin, begin + cnt) in strided passes.
-// Children are visited left before right and hits written by ballot rank,
-// so they come out in ascending tree position: the same set and order as
-// the packet walk (kdtree-impl.h:519-558).  Subtree start positions are
-// carried down the walk (a left child starts where its parent does, a right
-// child cnt[0] later) and checked against every leaf reached.
+// r-near walk with one warp per query, for batches too small to fill the
+// GPU as 32-query packets (a packet lane walks its own hits one by one, so a
+// few thousand queries with 1e4-1e5 hits each leave most of the GPU idle).
+// The warp walks its query's path once, with all lanes in step, and calls
+// visit(begin, n, whole) warp-uniformly for every leaf bucket the ball
+// touches and every child box inside the ball (whole = true: all of its
+// positions are hits), positions [begin, begin + n).  Children are visited
+// left before right, so the ranges come in ascending tree position, the
+// order of the reference's left-then-right walk (kdtree-impl.h:519-558).
+// Subtree start positions are carried down the walk (a left child starts
+// where its parent does, a right child cnt[0] later) and checked against
+// every leaf reached.  visit returns false to stop the walk; the result is
+// false then, or on a corrupt tree or a full stack.
+template <typename T, int D, typename DistT, typename Visit>
+__device__ __forceinline__ bool warp_rnear_walk(const TreeView<T, D>& tv, const DistT* q, DistT r2, int* stk,
+                                                int stack_ints, Visit visit) {
+  const int lane = threadIdx.x & 31;
+  bool bad = false;
+  // child c of nd, whose positions start at cb: visits it, or returns the
+  // inner node to descend into (-1: nothing to descend into)
+  auto take = [&](const TNode<T, D>& nd, int c, int cb) -> int {
+    const int n = nd.cnt[c];
+    if (n == 0 || !(box_min_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2)) return -1;
+    if (box_max_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2) {
+      if (!visit(cb, n, true)) bad = true;
+      return -1;
+    }
+    if (nd.ref[c] < 0) {
+      if (-nd.ref[c] - 1 != cb || !visit(cb, n, false)) bad = true;
+      return -1;
+    }
+    return nd.ref[c];
+  };
+  int sp = 0, cur = tv.root, b = 0, visits = 0;
+  while (!bad) {
+    if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
+      bad = true;
+      break;
+    }
+    const TNode<T, D> nd = load_node(tv.nodes, cur);
+    const int b1 = b + nd.cnt[0];
+    int next = take(nd, 0, b);
+    if (next >= 0) {
+      // into the left subtree; the right child waits if the ball reaches it
+      if (nd.cnt[1] > 0 && box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) < r2) {
+        if (2 * sp + 2 > stack_ints) {
+          bad = true;
+          break;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          stk[2 * sp] = cur * 2 + 1;
+          stk[2 * sp + 1] = b1;
+        }
+        __syncwarp();
+        sp++;
+      }
+      cur = next;
+      continue;
+    }
+    next = take(nd, 1, b1);
+    if (next >= 0) {
+      cur = next;
+      b = b1;
+      continue;
+    }
+    bool found = false;
+    while (sp > 0 && !bad) {
+      --sp;
+      const int e = stk[2 * sp], eb = stk[2 * sp + 1];
+      const int r = take(load_node(tv.nodes, e >> 1), e & 1, eb);
+      if (r >= 0) {
+        cur = r;
+        b = eb;
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return !bad;
+}
+
+// r-near counts or hit lists with one warp per query (warp_rnear_walk):
+// lane j tests position base + j of each chunk of a leaf bucket, a box
+// inside the ball is taken whole (the fill reads only its ids, the count adds
+// its size), and hits are written at their ballot rank, so they come out in
+// ascending tree position: the same set and order as the packet walk.
 // COUNT: counts[qid] = hits, the query's own point excluded as in
 // k_rnear_count; otherwise out[off[qid] ...] = original indices of the hits.
 template <typename T, int D, typename L, bool COUNT>
@@ -673,17 +750,20 @@ __global__ void __launch_bounds__(QTHREADS) k_rnear_warp(TreeView<T, D> tv, L ld
     wp = off[qid];
     wend = off[qid + 1];
   }
-  bool bad = false;
-  // positions [begin, begin + n): every one a hit (whole) or tested
-  auto run = [&](int begin, int n, bool whole) {
+  auto visit = [&](int begin, int n, bool whole) -> bool {
+    if (COUNT && whole) {
+      cnt += n;
+      return true;
+    }
+    bool bad = false;
     for (int base = begin; base < begin + n; base += 32) {
       const int p = base + lane;
       bool hit = false;
       int32_t id = 0;
       if (p < begin + n) {
         if (whole) {
-          hit = COUNT || p != own;
-          if (!COUNT && hit) id = tv.pts[p].id;
+          hit = p != own;
+          if (hit) id = tv.pts[p].id;
         } else {
           const PointRec<T, D> pr = tv.pts[p];
           hit = point_dist2<T, DistT, D>(pr.c, q) < r2 && (COUNT || p != own);
@@ -704,86 +784,15 @@ __global__ void __launch_bounds__(QTHREADS) k_rnear_warp(TreeView<T, D> tv, L ld
         wp += __popc(hm);
       }
     }
-    if (!COUNT) bad = __any_sync(FULL, bad);  // keep the walk's control flow warp-uniform
+    return !__any_sync(FULL, bad);  // warp-uniform
   };
-  // child c of nd, whose positions start at cb: scans or takes it, or
-  // returns the inner node to descend into (-1: nothing to descend into)
-  auto take = [&](const TNode<T, D>& nd, int c, int cb) -> int {
-    const int n = nd.cnt[c];
-    if (n == 0 || !(box_min_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2)) return -1;
-    if (box_max_dist2<T, DistT, D>(nd.lo[c], nd.hi[c], q) < r2) {
-      if (COUNT)
-        cnt += n;
-      else
-        run(cb, n, true);
-      return -1;
-    }
-    if (nd.ref[c] < 0) {
-      if (-nd.ref[c] - 1 != cb) {
-        bad = true;
-        return -1;
-      }
-      run(cb, n, false);
-      return -1;
-    }
-    return nd.ref[c];
-  };
-  if (active) {
-    int sp = 0, cur = tv.root, b = 0, visits = 0;
-    while (!bad) {
-      if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
-        bad = true;
-        break;
-      }
-      const TNode<T, D> nd = load_node(tv.nodes, cur);
-      const int b1 = b + nd.cnt[0];
-      int next = take(nd, 0, b);
-      if (next >= 0) {
-        // into the left subtree; the right child waits if the ball reaches it
-        if (nd.cnt[1] > 0 && box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) < r2) {
-          if (2 * sp + 2 > stack_ints) {
-            bad = true;
-            break;
-          }
-          __syncwarp();
-          if (lane == 0) {
-            stk[2 * sp] = cur * 2 + 1;
-            stk[2 * sp + 1] = b1;
-          }
-          __syncwarp();
-          sp++;
-        }
-        cur = next;
-        continue;
-      }
-      next = take(nd, 1, b1);
-      if (next >= 0) {
-        cur = next;
-        b = b1;
-        continue;
-      }
-      bool found = false;
-      while (sp > 0 && !bad) {
-        --sp;
-        const int e = stk[2 * sp], eb = stk[2 * sp + 1];
-        const int r = take(load_node(tv.nodes, e >> 1), e & 1, eb);
-        if (r >= 0) {
-          cur = r;
-          b = eb;
-          found = true;
-          break;
-        }
-      }
-      if (!found) break;
-    }
-  }
-  bad = __any_sync(FULL, bad);
+  const bool ok = !active || warp_rnear_walk<T, D, DistT>(tv, q, r2, stk, stack_ints, visit);
   if (lane != 0) return;
   if (COUNT) {
     if (own >= 0 && cnt > 0) cnt -= 1;  // the point itself is always a hit when r2 > 0
     counts[qid] = active ? cnt : 0;
-    if (bad) atomicExch(status, 1);
-  } else if (bad || wp != wend) {
+    if (!ok) atomicExch(status, 1);
+  } else if (!ok || wp != wend) {
     atomicExch(status, 2);
   }
 }
@@ -1083,6 +1092,82 @@ __global__ void __launch_bounds__(QTHREADS) k_normals_rnear(TreeView<T, 3> tv, L
   write_pca<T, double>(qid, (int)n, w, V, num_eigen, evecs, evals, sizes);
 }
 
+// k_normals_rnear with one warp per query (warp_rnear_walk), for batches
+// too small to fill the GPU as packets: each lane accumulates the shifted
+// FP64 sums of the hits it tests (boxes inside the ball are summed without
+// distance tests), the warp adds the lanes' sums, and lane 0 solves.  The
+// neighbourhood (every point within r, the query point included) and its
+// size are those of the packet kernel; the sums add in another order, so
+// results agree to FP64 rounding.
+template <typename T, typename L>
+__global__ void __launch_bounds__(QTHREADS) k_normals_rnear_warp(TreeView<T, 3> tv, L ld, const int* order,
+                                                                 int order_mode, int m, typename DistOf<T>::type r2,
+                                                                 int stack_ints, int num_eigen, T* evecs, T* evals,
+                                                                 int32_t* sizes, int* status) {
+  typedef typename DistOf<T>::type DistT;
+  extern __shared__ __align__(16) int rw_stack[];
+  const int w = blockIdx.x * QWARPS + (threadIdx.x >> 5);
+  if (w >= m) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xffffffffu;
+  int* stk = rw_stack + (threadIdx.x >> 5) * stack_ints;
+  const int qid = query_of(w, order, order_mode, tv);
+  DistT q[3];
+  int own = -1;
+  const bool active = ld.load(qid, tv, q, own);
+  double s[3] = {0, 0, 0}, ss[6] = {0, 0, 0, 0, 0, 0};
+  long long n = 0;
+  auto visit = [&](int begin, int cnt, bool whole) -> bool {
+    for (int base = begin; base < begin + cnt; base += 32) {
+      const int p = base + lane;
+      if (p >= begin + cnt) continue;
+      const PointRec<T, 3> pr = tv.pts[p];
+      if (!whole && !(point_dist2<T, DistT, 3>(pr.c, q) < r2)) continue;
+      const double e0 = (double)pr.c[0] - (double)q[0], e1 = (double)pr.c[1] - (double)q[1],
+                   e2 = (double)pr.c[2] - (double)q[2];
+      s[0] += e0;
+      s[1] += e1;
+      s[2] += e2;
+      ss[0] += e0 * e0;
+      ss[1] += e0 * e1;
+      ss[2] += e0 * e2;
+      ss[3] += e1 * e1;
+      ss[4] += e1 * e2;
+      ss[5] += e2 * e2;
+      n++;
+    }
+    __syncwarp();
+    return true;
+  };
+  const bool ok = !active || warp_rnear_walk<T, 3, DistT>(tv, q, r2, stk, stack_ints, visit);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) s[d] += __shfl_xor_sync(FULL, s[d], o);
+#pragma unroll
+    for (int d = 0; d < 6; d++) ss[d] += __shfl_xor_sync(FULL, ss[d], o);
+    n += __shfl_xor_sync(FULL, n, o);
+  }
+  if (lane != 0) return;
+  if (!ok) atomicExch(status, 1);
+  if (!active || n == 0) {
+    write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
+    return;
+  }
+  const double inv = 1.0 / (double)n;
+  const double m0 = s[0] * inv, m1 = s[1] * inv, m2 = s[2] * inv;
+  Sym3<double> C;
+  C.a00 = ss[0] * inv - m0 * m0;
+  C.a01 = ss[1] * inv - m0 * m1;
+  C.a02 = ss[2] * inv - m0 * m2;
+  C.a11 = ss[3] * inv - m1 * m1;
+  C.a12 = ss[4] * inv - m1 * m2;
+  C.a22 = ss[5] * inv - m2 * m2;
+  double wv[3], V[9];
+  eigh3<double>(C, wv, V);
+  write_pca<T, double>(qid, (int)n, wv, V, num_eigen, evecs, evals, sizes);
+}
+
 // FP64 re-solve of queued neighbourhoods: one thread per entry, a gather of
 // the stored neighbour positions, float64 covariance (shifted to the first
 // neighbour, centred) and eigensolve; overwrites the FP32 results of that
@@ -1283,7 +1368,16 @@ void normals_query(const TreeBase* t, const QuerySpec& qs_in, int k, float r, in
   const DistT r2 = rr * rr;
   IndexQueries<3, false> ld{qs.idx, t->fwd};
   Stage stage("normals", st);
-  if (k == -1) {
+  if (k == -1 && m <= g_tune_rnear_warp_queries.load()) {
+    const int si = rnear_warp_stack_ints(t->tdepth);
+    const size_t smem = (size_t)QWARPS * si * sizeof(int);
+    if (smem > 48 * 1024)
+      PPTKG_CUDA(cudaFuncSetAttribute(k_normals_rnear_warp<T, IndexQueries<3, false>>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_normals_rnear_warp<T, IndexQueries<3, false>><<<div_up(m, QWARPS), QTHREADS, smem, st>>>(
+        view_of<T, 3>(t), ld, order.get(), mode, m, r2, si, num_eigen, d_evecs, d_evals, d_sizes, status.get());
+    PPTKG_CHECK_LAUNCH();
+  } else if (k == -1) {
     const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth);
     if (smem > 48 * 1024)
       PPTKG_CUDA(cudaFuncSetAttribute(k_normals_rnear<T, IndexQueries<3, false>>,

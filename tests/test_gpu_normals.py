@@ -130,6 +130,38 @@ def test_normals_with_radius_and_rnear_neighbourhoods(gpu, port):
     assert (angle_error(ev[ok, 0], pev[ok, 0]) < 2e-3).all()
 
 
+def test_rnear_normals_warp_per_query_matches_packets(gpu):
+    # r-near neighbourhoods (k = -1) of small batches run one warp per query
+    # (rnear_warp_queries); sizes must match the packet walk exactly and the
+    # FP64-solved normals and eigenvalues to rounding, for all points and a
+    # subsample
+    from pptk_b200 import _native as N
+    P = np.random.default_rng(6).random((30_000, 3)).astype(np.float32)
+    sub = np.arange(0, len(P), 7, dtype=np.int64)
+    default = N.tune_get("rnear_warp_queries")
+    out = {}
+    try:
+        for wq in (0, 1 << 30):
+            N.tune_set("rnear_warp_queries", wq)
+            out[wq] = (gpu.estimate_normals(P, -1, 0.04, output_eigenvalues=True, output_all_eigenvectors=True,
+                                            output_neighborhood_sizes=True, verbose=False),
+                       gpu.estimate_normals(P, -1, 0.04, subsample=sub, output_eigenvalues=True,
+                                            output_all_eigenvectors=True, output_neighborhood_sizes=True,
+                                            verbose=False))
+    finally:
+        N.tune_set("rnear_warp_queries", default)
+    (ev0, ew0, sz0), (sv0, sw0, ss0) = out[0]
+    (ev1, ew1, sz1), (sv1, sw1, ss1) = out[1 << 30]
+    assert np.array_equal(sz0, sz1) and np.array_equal(ss0, ss1)
+    ok = sz0 >= 5
+    ok &= (ew0[:, 1] - ew0[:, 0]) / np.maximum(ew0[:, 2], 1e-30) > 1e-3
+    assert (angle_error(ev0[ok, 0], ev1[ok, 0]) < 1e-5).all()
+    np.testing.assert_allclose(ew0[ok], ew1[ok], rtol=1e-5, atol=1e-9)
+    oks = ss0 >= 5
+    oks &= (sw0[:, 1] - sw0[:, 0]) / np.maximum(sw0[:, 2], 1e-30) > 1e-3
+    assert (angle_error(sv0[oks, 0], sv1[oks, 0]) < 1e-5).all()
+
+
 def test_precision_split_on_offset_planes(gpu):
     # config-3 shape, reduced: thin patches 1e5 m from the origin, float64
     from pptk_b200 import synth
