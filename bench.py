@@ -19,7 +19,8 @@ the whole stream (40M queries).
   tree on every call, as the reference does); device inputs, and host numpy
   inputs for ``plain.e2e``.  Timed on a bounded sample of the stream.
 * ``latency``: p50/p99 request latency of the server under Poisson arrivals
-  at half of the measured serving throughput, and of the plain calls.
+  at half of the measured serving throughput (``latency_at_quarter_load``:
+  at a quarter), and of the plain calls.
 * ``e2e``: the serving form through its public API with pinned host numpy
   inputs and numpy results (host<->device copies inside the timed region).
 * ``roofline``: the fused kNN+PCA normal kernel's algorithmic bytes (216 B
@@ -712,33 +713,38 @@ def run_serving_workload(args, ctx):
     ms_max = ctx.max_over_ranks(ms)
     value = ctx.throughput(per_step, ms / 1e3)
 
-    # latency at a fixed offered load: Poisson arrivals at half the measured
-    # serving throughput, requests drawn in stream order
-    rng = np.random.default_rng(12)
-    offered = 0.5 * per_step / (ms_max / 1e3)
-    mean_m = per_step / len(mix_dev)
-    t_start = time.perf_counter()
-    futs, i = [], 0
-    next_t = t_start
-    while time.perf_counter() - t_start < args.latency_seconds:
-        now = time.perf_counter()
-        if now < next_t:
-            time.sleep(min(next_t - now, 0.002))
-            continue
-        kind, a = mix_dev[i % len(mix_dev)]
-        futs.append(srv.knn(tid, a, k=k) if kind == "knn" else srv.normals(tid, a, k=k))
-        i += 1
-        next_t += rng.exponential(mean_m / offered)
-    for f in futs:
-        f.result()
-    st = srv.stats(since=t_start)
-    with srv._cv:
-        lat_all = [d[3] - d[2] for d in srv._done if d[2] >= t_start and d[0] in ("knn", "normals")]
-    latency = {"offered_queries_per_s": offered, "arrivals": "poisson",
-               "serving": percentiles(lat_all),
-               "serving_by_kind": {kk: {"p50_ms": v["p50_s"] * 1e3, "p99_ms": v["p99_s"] * 1e3,
-                                        "requests": v["requests"]}
-                                   for kk, v in st.items() if isinstance(v, dict)}}
+    # latency at fixed offered loads: Poisson arrivals at half (`latency`)
+    # and a quarter (`latency_at_quarter_load`) of the measured serving
+    # throughput, requests drawn in stream order
+    def poisson_latency(frac, seed):
+        rng = np.random.default_rng(seed)
+        offered = frac * per_step / (ms_max / 1e3)
+        mean_m = per_step / len(mix_dev)
+        t_start = time.perf_counter()
+        futs, i = [], 0
+        next_t = t_start
+        while time.perf_counter() - t_start < args.latency_seconds:
+            now = time.perf_counter()
+            if now < next_t:
+                time.sleep(min(next_t - now, 0.002))
+                continue
+            kind, a = mix_dev[i % len(mix_dev)]
+            futs.append(srv.knn(tid, a, k=k) if kind == "knn" else srv.normals(tid, a, k=k))
+            i += 1
+            next_t += rng.exponential(mean_m / offered)
+        for f in futs:
+            f.result()
+        st = srv.stats(since=t_start)
+        with srv._cv:
+            lat_all = [d[3] - d[2] for d in srv._done if d[2] >= t_start and d[0] in ("knn", "normals")]
+        return {"offered_queries_per_s": offered, "arrivals": "poisson",
+                "serving": percentiles(lat_all),
+                "serving_by_kind": {kk: {"p50_ms": v["p50_s"] * 1e3, "p99_ms": v["p99_s"] * 1e3,
+                                         "requests": v["requests"]}
+                                    for kk, v in st.items() if isinstance(v, dict)}}
+
+    latency = poisson_latency(0.5, 12)
+    latency_q = poisson_latency(0.25, 13)
 
     # plain per-call drop-in on a bounded sample of the same stream
     tree = kdtree._build(dev)
@@ -810,7 +816,7 @@ def run_serving_workload(args, ctx):
                        "slots": args.slots, "max_batch_queries": args.max_batch,
                        "l2": "scene (240 MB) and request inputs larger than L2 (126 MB); no flush",
                        "parallelism": f"replicas x{ctx.world}"},
-            "plain": plain, "latency": latency,
+            "plain": plain, "latency": latency, "latency_at_quarter_load": latency_q,
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk}
 
