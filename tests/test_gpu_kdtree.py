@@ -149,6 +149,27 @@ def test_rnear_warp_per_query_matches_packets_and_oracle(gpu, port, dtype, dim):
             N.tune_set("rnear_warp_queries", wq)
             off, out = gpu.kdtree.rnear(t, None, r)
             assert np.array_equal(off, aoff) and np.array_equal(out, aout), wq
+        # edge cases: an empty tree, one point, every point identical
+        if dtype == np.float32 and dim == 3:
+            for E in (np.zeros((0, 3), np.float32), np.array([[0.5, 0.5, 0.5]], np.float32),
+                      np.ones((300, 3), np.float32)):
+                te = gpu.kdtree._build(E)
+                qe = np.array([[0.5, 0.5, 0.5], [1.0, 1.0, 1.0], [9.0, 9.0, 9.0]], np.float32)
+                got = []
+                for wq in (0, 1 << 30):
+                    N.tune_set("rnear_warp_queries", wq)
+                    got.append(gpu.kdtree.rnear(te, qe, 0.6))
+                    if len(E):
+                        got.append(gpu.kdtree.rnear(te, np.arange(len(E), dtype=np.int32), 0.6))
+                half = len(got) // 2
+                for a, b in zip(got[:half], got[half:]):
+                    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                if len(E):
+                    oe = port.PortTree(E)
+                    ooff, oout = oe.rnear(qe, float(np.float32(0.6)))
+                    assert np.array_equal(got[0][0], ooff) and np.array_equal(got[0][1], oout)
+                else:
+                    assert (got[0][0] == 0).all() and len(got[0][1]) == 0
     finally:
         N.tune_set("rnear_warp_queries", default)
 
