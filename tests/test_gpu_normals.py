@@ -160,6 +160,19 @@ def test_rnear_normals_warp_per_query_matches_packets(gpu):
     oks = ss0 >= 5
     oks &= (sw0[:, 1] - sw0[:, 0]) / np.maximum(sw0[:, 2], 1e-30) > 1e-3
     assert (angle_error(sv0[oks, 0], sv1[oks, 0]) < 1e-5).all()
+    # rows with NaN coordinates: size 0 and NaN results in both forms
+    P2 = P[:3000].copy()
+    P2[::97] = np.nan
+    res = []
+    try:
+        for wq in (0, 1 << 30):
+            N.tune_set("rnear_warp_queries", wq)
+            res.append(gpu.estimate_normals(P2, -1, 0.05, output_neighborhood_sizes=True, verbose=False))
+    finally:
+        N.tune_set("rnear_warp_queries", default)
+    (n0, _, z0), (n1, _, z1) = res
+    assert np.array_equal(z0, z1) and (z0[::97] == 0).all()
+    assert np.array_equal(np.isnan(n0), np.isnan(n1)) and np.isnan(n0[::97]).all()
 
 
 def test_precision_split_on_offset_planes(gpu):
