@@ -105,10 +105,11 @@ PPTKG_API int pptkg_tree_set_bucket(pptkg_tree* tree, int bucket, void* stream);
 
 /* k nearest neighbours of m point queries (rows of `dim` coordinates of
  * qdtype F32/F64) with distance < dmax.  out_idx: m x k original row indices
- * in ascending distance (ties: ascending tree position), -1 padded; out_cnt
- * (optional): neighbours found.  Replaces QueryWithPoints with k > 0
- * (kdtree_wrapper.cpp:139-159) / KdTree::KNearestNeighbors
- * (kdtree-impl.h:873-929).  1 <= k <= 64. */
+ * in ascending distance, ties in distance broken by ascending original
+ * index, -1 padded; out_cnt (optional): neighbours found.  Replaces
+ * QueryWithPoints with k > 0 (kdtree_wrapper.cpp:139-159) /
+ * KdTree::KNearestNeighbors (kdtree-impl.h:873-929).  k >= 1 (above 64 the
+ * lists live in device-memory heaps). */
 PPTKG_API int pptkg_knn(const pptkg_tree* tree, const void* queries, int64_t m, int qdtype, int mem, int k, double dmax,
               int32_t* out_idx, int32_t* out_cnt, void* stream);
 

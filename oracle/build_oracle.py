@@ -17,7 +17,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("PPTK_REFERENCE", "/root/reference")
+# the reference source tree: $PPTK_REFERENCE, else a `reference` directory
+# beside the repository
+REF_SRC = os.environ.get("PPTK_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 FLAGS = ["-O3", "-DNDEBUG", "-std=c++14", "-fopenmp", "-shared", "-fPIC"]
 
 

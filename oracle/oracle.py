@@ -150,7 +150,7 @@ class PortTree(_Tree):
         return out
 
     def knn(self, q, k, dmax=np.inf, nthreads=0, with_pos=False):
-        """(idx m x k, cnt m[, pos m x k, d2 m x k]) in (dist2, tree position) order."""
+        """(idx m x k, cnt m[, pos m x k, d2 m x k]) in (dist2, point index) order."""
         q = self._queries(q)
         m = q.shape[0]
         idx = np.empty((m, k), np.int32)

@@ -6,12 +6,13 @@
 // Every function cites the reference code it restates (paths relative to
 // the pptk project).  Two semantics are deliberately pinned here, and the
 // GPU path follows the same ones:
-//  * kNN results are the k smallest (dist2, tree position) pairs among the
-//    points with dist2 < r^2, in that order.  The reference keeps whichever
-//    equal-dist2 candidate its std::priority_queue happens to keep
-//    (kdtree-impl.h:360-373, :894-899); outside of exact distance ties the
-//    two agree, and the tests compare against the reference after sorting
-//    each equal-dist2 run by tree position.
+//  * kNN results are the k smallest (dist2, original index) pairs among the
+//    points with dist2 < r^2, in that order: ties in distance are broken by
+//    point index.  The reference keeps whichever equal-dist2 candidate its
+//    std::priority_queue happens to keep (kdtree-impl.h:360-373, :894-899);
+//    outside of exact distance ties the two agree, and the tests compare
+//    against the reference after sorting each equal-dist2 run and allowing
+//    the choice among points tied at the k-th distance.
 //  * eigenvectors are signed so that their largest-magnitude component is
 //    positive (Eigen's sign is an implementation artefact; the reference's
 //    own test pins only +[1,0,0] on collinear input, which this convention
@@ -315,15 +316,15 @@ Tree<T, D>* build(const T* P, int64_t n, int max_leaf, double thr) {
   return t;
 }
 
-// Sorted candidate list of (dist2, tree position), at most k long.
+// Sorted candidate list of (dist2, original index), at most k long.
 template <typename DistT>
 struct TopK {
   int k;
   std::vector<std::pair<DistT, int>> v;
   bool full() const { return (int)v.size() >= k; }
   DistT worst() const { return v.back().first; }
-  void offer(DistT d, int pos) {
-    std::pair<DistT, int> c(d, pos);
+  void offer(DistT d, int id) {
+    std::pair<DistT, int> c(d, id);
     if (full() && !(c < v.back())) return;
     auto it = std::upper_bound(v.begin(), v.end(), c);
     v.insert(it, c);
@@ -334,7 +335,7 @@ struct TopK {
 // Near-child-first depth-first kNN over the same tree and the same loose
 // node extents as KNearestNeighborsHelper (kdtree-impl.h:348-429), with the
 // far child visited while its box can still hold a candidate that ties or
-// beats the current k-th (dist2, position).
+// beats the current k-th (dist2, index).
 template <typename T, int D, typename Q>
 void knn_rec(const Tree<T, D>& t, int node, int b, int e, Box<T, D>& box, const Q* q,
              typename Tree<T, D>::DistT r2, TopK<typename Tree<T, D>::DistT>& top) {
@@ -342,7 +343,7 @@ void knn_rec(const Tree<T, D>& t, int node, int b, int e, Box<T, D>& box, const 
   if (node < 0) {
     for (int i = b; i < e; i++) {
       DistT d2 = point_dist2<DistT, Q, T, D>(q, &t.pts[(size_t)i * D]);
-      if (d2 < r2) top.offer(d2, i);
+      if (d2 < r2) top.offer(d2, t.rev[i]);
     }
     return;
   }
@@ -537,8 +538,8 @@ void port_knn(void* hp, const void* q, int64_t m, int qdtype, int k, double dmax
         knn_one<T, D, Q>(tr, qp + i * D, k, (DistT)dmax, res);
         for (int j = 0; j < k; j++) {
           bool ok = j < (int)res.size();
-          out_idx[i * k + j] = ok ? tr.rev[res[j].second] : -1;
-          if (out_pos) out_pos[i * k + j] = ok ? res[j].second : -1;
+          out_idx[i * k + j] = ok ? res[j].second : -1;
+          if (out_pos) out_pos[i * k + j] = ok ? tr.fwd[res[j].second] : -1;
           if (out_d2) out_d2[i * k + j] = ok ? (double)res[j].first : -1.0;
         }
         out_cnt[i] = (int32_t)res.size();
@@ -566,7 +567,7 @@ void port_knn_self(void* hp, const int32_t* qidx, int64_t m, int k, double dmax,
         std::vector<std::pair<DistT, int>> res;
         knn_one<T, D, T>(tr, &tr.pts[(size_t)tr.fwd[qi] * D], k + 1, (DistT)dmax, res);
         for (size_t j = 0; j < res.size() && cnt < k; j++) {
-          int oi = tr.rev[res[j].second];
+          int oi = res[j].second;
           if (oi != qi) out_idx[i * k + cnt++] = oi;
         }
       }
@@ -660,7 +661,7 @@ void port_estimate_normals(const void* pts, int64_t n, int dtype, int k, float r
       } else {
         std::vector<std::pair<DistT, int>> res;
         knn_one<T, 3, T>(*tr, q, k, (DistT)(T)r, res);
-        for (auto& pr : res) nb.push_back(tr->rev[pr.second]);
+        for (auto& pr : res) nb.push_back(pr.second);
       }
       if (nbr_idx && k > 0)
         for (int j = 0; j < k; j++) nbr_idx[i * k + j] = j < (int)nb.size() ? nb[j] : -1;

@@ -58,14 +58,19 @@ __device__ __forceinline__ DistT box_max_dist2(const T* lo, const T* hi, const D
 }
 
 // ---------------------------------------------------------------- top-k ---
-// The k best (dist2, tree position) pairs, held in registers in descending
-// order so that the current k-th best is always slot 0.  KMAX is the compile
-// time capacity; for a run-time k < KMAX the slots [k, KMAX) hold entries
-// that compare below every candidate and never move.
+// The k best (dist2, point id) pairs, held in registers in descending order
+// so that the current k-th best is always slot 0.  The id is the point's
+// original index, so among equal distances the smaller index wins -- both
+// for the order of a result and for which point takes the k-th slot.  (The
+// reference keeps whichever equal-distance candidate its std::priority_queue
+// happens to retain, kdtree-impl.h:360-373, 894-899; an index order makes the
+// answer a function of the input alone.)  KMAX is the compile time capacity;
+// for a run-time k < KMAX the slots [k, KMAX) hold entries that compare below
+// every candidate and never move.
 template <int KMAX, typename DistT>
 struct TopK;
 
-// float distances: (dist2 bits << 32 | position) packed into one 64-bit key;
+// float distances: (dist2 bits << 32 | id) packed into one 64-bit key;
 // non-negative floats order like their bit patterns.
 template <int KMAX>
 struct TopK<KMAX, float> {
@@ -77,8 +82,8 @@ struct TopK<KMAX, float> {
     for (int j = 0; j < KMAX; j++) s[j] = j < k ? lim : 0ull;
   }
   __device__ __forceinline__ float worst() const { return __uint_as_float((unsigned)(s[0] >> 32)); }
-  __device__ __forceinline__ void offer(float d2, int pos) {
-    unsigned long long c = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)pos;
+  __device__ __forceinline__ void offer(float d2, int id) {
+    unsigned long long c = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
     if (c < s[0]) insert(c);
   }
   __device__ __forceinline__ void insert(unsigned long long c) {
@@ -102,11 +107,11 @@ struct TopK<KMAX, float> {
   }
   __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return s[j] < lim && (unsigned)s[j] != 0xffffffffu; }
-  __device__ __forceinline__ int pos(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
+  __device__ __forceinline__ int id(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
   __device__ __forceinline__ float dist(int j) const { return __uint_as_float((unsigned)(s[j] >> 32)); }
 };
 
-// double distances: parallel (dist2, position) arrays compared lexicographically.
+// double distances: parallel (dist2, id) arrays compared lexicographically.
 template <int KMAX>
 struct TopK<KMAX, double> {
   double d[KMAX];
@@ -122,8 +127,8 @@ struct TopK<KMAX, double> {
   __device__ __forceinline__ static bool gt(double da, int pa, double db, int pb) {
     return da > db || (da == db && pa > pb);
   }
-  __device__ __forceinline__ void offer(double d2, int pos) {
-    if (gt(d[0], p[0], d2, pos)) insert(d2, pos);
+  __device__ __forceinline__ void offer(double d2, int id) {
+    if (gt(d[0], p[0], d2, id)) insert(d2, id);
   }
   __device__ __forceinline__ void insert(double cd, int cp) {
 #pragma unroll
@@ -150,7 +155,7 @@ struct TopK<KMAX, double> {
   }
   __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && p[j] != 0x7fffffff && d[j] >= 0.0; }
-  __device__ __forceinline__ int pos(int j) const { return p[j]; }
+  __device__ __forceinline__ int id(int j) const { return p[j]; }
   __device__ __forceinline__ double dist(int j) const { return d[j]; }
 };
 
@@ -162,6 +167,7 @@ struct WarpScratch {
   PointRec<T, D>* buf;                   // 32 entries (r-near staging)
   int* log;                              // per-lane neighbour lists, lane-strided; null when unused
   typename DistOf<T>::type* dmat;        // 32 x 33 distances (kNN bucket scan); null when unused
+  int* cid;                              // 32 candidate ids of the chunk being scanned (kNN)
 };
 
 // A lane's query as the rest of its warp reads it during a bucket scan:
@@ -212,7 +218,7 @@ __device__ __forceinline__ TNode<T, D> load_node(const TNode<T, D>* nodes, int i
 }
 
 // Exact kNN of the lane's query over the whole tree, ties in dist2 broken by
-// tree position.  `own` (tree position or -1) is skipped, which is how self
+// point id.  `own` (tree position or -1) is skipped, which is how self
 // queries exclude the query point itself.  Returns false when the traversal
 // stack would overflow (the host sizes it from the tree depth, so this is a
 // safety net that reports instead of corrupting memory).
@@ -235,7 +241,8 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
   // query needs this bucket.  For such a query i every lane computes its
   // candidate's distance to q_i; the row goes to dmat[i][*] and the ballot of
   // candidates that can enter list i becomes lane i's mark mask.  Each lane
-  // then inserts its marked candidates, reading distances from its row.
+  // then inserts its marked candidates, reading distances from its row and
+  // the candidates' ids from the chunk's id row.
   // The queries sit in the warp's staging buffer (unused by kNN walks) so
   // that lane i's coordinates and bound arrive as one shared broadcast.
   QStage<DistT, D>* qst = reinterpret_cast<QStage<DistT, D>*>(ws.buf);
@@ -252,11 +259,13 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
       } else {
 #pragma unroll
         for (int d = 0; d < D; d++) pr.c[d] = (T)0;
+        pr.id = -1;
       }
       // each needing lane publishes its entry bound for this chunk; the
       // loop below reads a query and its bound as one broadcast
       __syncwarp();
       qst[lane].thr = entry_bound(top.worst(), r2_below);
+      ws.cid[lane] = pr.id;
       __syncwarp();
       const unsigned valid = nb == 32 ? FULL : (1u << nb) - 1u;
       unsigned mark = 0;
@@ -277,7 +286,7 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
       while (mark) {
         const int t = __ffs(mark) - 1;
         mark &= mark - 1;
-        top.offer(ws.dmat[lane * 33 + t], base + t);
+        top.offer(ws.dmat[lane * 33 + t], ws.cid[t]);
       }
       __syncwarp();
     }
@@ -381,7 +390,7 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
 // the 32 walks advance side by side and their node loads overlap.  The set of
 // candidates each query accepts is the same as in the packet walk: every
 // point whose distance is within the query's final bound is offered, so the
-// result (the k smallest (dist2, position) pairs) is identical.
+// result (the k smallest (dist2, id) pairs) is identical.
 // Requires tv.depth <= LSTACK (the caller checks); false on a corrupt tree.
 template <int LSTACK, typename T, int D, typename DistT, typename Top>
 __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top) {
@@ -396,16 +405,21 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
     const int end = begin + count;
     int p = begin;
     for (; p + 4 <= end; p += 4) {
+      PointRec<T, D> r[4];
       DistT d2[4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) d2[j] = point_dist2<T, DistT, D>(tv.pts[p + j].c, q);
+      for (int j = 0; j < 4; j++) {
+        r[j] = tv.pts[p + j];
+        d2[j] = point_dist2<T, DistT, D>(r[j].c, q);
+      }
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        if (d2[j] <= top.worst() && d2[j] < r2 && p + j != own) top.offer(d2[j], p + j);
+        if (d2[j] <= top.worst() && d2[j] < r2 && p + j != own) top.offer(d2[j], r[j].id);
     }
     for (; p < end; p++) {
-      const DistT d2 = point_dist2<T, DistT, D>(tv.pts[p].c, q);
-      if (d2 <= top.worst() && d2 < r2 && p != own) top.offer(d2, p);
+      const PointRec<T, D> r = tv.pts[p];
+      const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
+      if (d2 <= top.worst() && d2 < r2 && p != own) top.offer(d2, r.id);
     }
   };
   int cur = tv.root, visits = 0;
@@ -455,8 +469,8 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
 }
 
 // Top-k of any size k for the per-lane walk: a binary max-heap of
-// (dist2, position) pairs in device memory, ordered like the register lists
-// ((dist2, position) lexicographic), so the k kept are the same k smallest.
+// (dist2, id) pairs in device memory, ordered like the register lists
+// ((dist2, id) lexicographic), so the k kept are the same k smallest.
 // Slot 0 holds the current k-th once the heap is full.
 template <typename DistT>
 struct HeapTop {
@@ -483,21 +497,21 @@ struct HeapTop {
     d[i] = di;
     p[i] = pi;
   }
-  __device__ void offer(DistT d2, int pos) {
+  __device__ void offer(DistT d2, int id) {
     if (size < k) {
       int i = size++;
       while (i > 0) {
         const int par = (i - 1) / 2;
-        if (!gt(d2, pos, d[par], p[par])) break;
+        if (!gt(d2, id, d[par], p[par])) break;
         d[i] = d[par];
         p[i] = p[par];
         i = par;
       }
       d[i] = d2;
-      p[i] = pos;
-    } else if (gt(d[0], p[0], d2, pos)) {
+      p[i] = id;
+    } else if (gt(d[0], p[0], d2, id)) {
       d[0] = d2;
-      p[0] = pos;
+      p[0] = id;
       sift_down(0, size);
     }
   }

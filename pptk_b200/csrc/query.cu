@@ -32,7 +32,8 @@ TreeView<T, D> view_of(const TreeBase* t) {
 
 // Per-warp shared memory: the staging buffer (a leaf chunk in r-near walks,
 // the warp's queries in kNN walks), traversal stack, the 32 x 33 distance
-// matrix of the kNN bucket scan, and (normals) `logcap` list slots per lane.
+// matrix and the 32 candidate ids of the kNN bucket scan, and (normals)
+// `logcap` list slots per lane.
 template <typename T, int D>
 __host__ __device__ constexpr size_t stage_bytes() {
   typedef typename DistOf<T>::type DistT;
@@ -43,7 +44,7 @@ template <typename T, int D>
 __host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
   return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
-         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + (size_t)logcap * 32 * 4;
+         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4 + (size_t)logcap * 32 * 4;
 }
 
 template <typename T, int D>
@@ -59,6 +60,8 @@ __device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap 
   base += ((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15;
   ws.dmat = (DistT*)base;
   base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
+  ws.cid = (int*)base;
+  base += 32 * 4;
   ws.log = logcap ? (int*)base : nullptr;
   return ws;
 }
@@ -413,7 +416,7 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
       if (j < k) {
         const bool v = active && top.valid(j);
         c += v;
-        out_idx[(int64_t)qid * k + (k - 1 - j)] = v ? tv.pts[top.pos(j)].id : -1;
+        out_idx[(int64_t)qid * k + (k - 1 - j)] = v ? top.id(j) : -1;
       }
     }
     if (out_cnt) out_cnt[qid] = c;
@@ -491,8 +494,8 @@ struct StatusWord {
 // at slot `m0` of the processing order; hd / hp hold one heap per slot.
 constexpr int BIG_STACK = 128;
 
-// POS: write tree positions to chunk rows (for the normal pass) instead of
-// original indices to query rows.
+// POS: write tree positions (through the tree's index map) to chunk rows
+// (for the normal pass) instead of original indices to query rows.
 template <typename T, int D, typename L, bool POS>
 __global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m0, int m, int k,
                           typename DistOf<T>::type r2, typename DistOf<T>::type* hd, int* hp, int32_t* out_idx,
@@ -509,7 +512,7 @@ __global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_m
   top.sort();
   const int64_t row = POS ? i : qid;
   int32_t* out = out_idx + row * k;
-  for (int j = 0; j < k; j++) out[j] = j < top.size ? (POS ? top.p[j] : tv.pts[top.p[j]].id) : -1;
+  for (int j = 0; j < k; j++) out[j] = j < top.size ? (POS ? tv.fwd[top.p[j]] : top.p[j]) : -1;
   if (out_cnt) out_cnt[row] = top.size;
 }
 
@@ -1013,10 +1016,12 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
     return;
   }
+  // the list holds point ids; the neighbours are gathered from their tree
+  // positions (the index map's loads are independent and overlap)
   int n = 0;
 #pragma unroll
   for (int j = KMAX - 1; j >= 0; j--)
-    if (j < k && top.valid(j)) lane_log[(n++) * 32] = top.pos(j);
+    if (j < k && top.valid(j)) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
   if (PREC == PREC_FP64) {
     Sym3<double> C = log_covariance<T, double, DistT>(tv, lane_log, n, q);
     double w[3], V[9];

@@ -5,8 +5,9 @@ import numpy as np
 def dist2(P, Q, idx):
     """Squared distances of result rows, computed as the reference does
     (kdtree-impl.h:331-339): per-axis (point - query) in the distance type
-    (float32 for float32 trees, float64 for float64), squared, summed in
-    axis order with one rounding per operation.  -1 indices give inf."""
+    (float32 for float32 and integer trees, float64 for float64), squared,
+    summed in axis order with one rounding per operation.  -1 indices give
+    inf."""
     dt = np.float64 if P.dtype == np.float64 else np.float32
     P = P.astype(dt, copy=False)
     Q = np.asarray(Q).astype(dt, copy=False)
@@ -19,22 +20,53 @@ def dist2(P, Q, idx):
     return np.where(idx >= 0, s, np.inf)
 
 
-def canonical_rows(idx, d2, pos_of):
-    """Sorts each row by (dist2, tree position); -1 entries stay last."""
-    pos = np.where(idx >= 0, pos_of[np.where(idx >= 0, idx, 0)], np.iinfo(np.int64).max)
-    order = np.lexsort((pos, d2), axis=-1)
+def canonical_rows(idx, d2):
+    """Sorts each row by (dist2, point index); -1 entries stay last."""
+    key = np.where(idx >= 0, idx, np.iinfo(np.int32).max).astype(np.int64)
+    order = np.lexsort((key, d2), axis=-1)
     return np.take_along_axis(idx, order, -1), np.take_along_axis(d2, order, -1)
 
 
-def compare_knn(got, got_cnt, exp, exp_cnt, P, Q, pos_of, k):
-    """Compares kNN results allowing only the reference's tie freedom.
+def brute_knn(P, Q, k, dmax=np.inf, exclude=None):
+    """The specified kNN answer by exhaustive search: the k smallest
+    (dist2, point index) pairs among the valid points with dist2 < dmax^2,
+    dist2 in the reference's arithmetic.  exclude[i] (optional) is an index
+    left out of row i (self queries).  NaN/inf rows of P are never answers.
+    Returns (idx m x k, -1 padded; cnt m)."""
+    P = np.asarray(P)
+    Q = np.asarray(Q)
+    m, n = len(Q), len(P)
+    dt = np.float64 if P.dtype == np.float64 else np.float32
+    r = dt(dmax)
+    r2 = r * r
+    valid = np.isfinite(P.astype(np.float64)).all(1)
+    idx = np.full((m, k), -1, np.int32)
+    cnt = np.zeros(m, np.int32)
+    allidx = np.arange(n)[None, :]
+    for i in range(m):
+        d = dist2(P, Q[i:i + 1], allidx)[0]
+        ok = valid & (d < r2)
+        if exclude is not None and exclude[i] >= 0:
+            ok[exclude[i]] = False
+        cand = np.flatnonzero(ok)
+        sel = cand[np.lexsort((cand, d[cand]))][:k]
+        idx[i, :len(sel)] = sel
+        cnt[i] = len(sel)
+    return idx, cnt
 
-    Both sides are canonicalised to (dist2, tree position) order.  They must
-    agree exactly, except inside the final run of equal dist2 of a full
-    result (a tie at the k-th distance), where the reference keeps whichever
-    tied point its heap retained; there both sides must hold points of that
-    same distance.  Returns (rows that differ beyond that, rows with a
-    k-boundary tie choice that differs)."""
+
+def compare_knn(got, got_cnt, exp, exp_cnt, P, Q, k):
+    """Compares a kNN result with the reference's, allowing only the
+    reference's tie freedom.
+
+    The reference keeps whichever equal-distance candidate its heap retains
+    (kdtree-impl.h:360-373, 894-899), so its order inside a run of equal
+    dist2, and its choice among points tied at the k-th distance, are
+    arbitrary.  Both sides are canonicalised to (dist2, index) order and must
+    then agree exactly, except inside the final run of equal dist2 of a full
+    result, where both sides must hold points of that same distance.
+    Returns (rows that differ beyond that, rows with a k-boundary tie choice
+    that differs)."""
     got = np.asarray(got)
     exp = np.asarray(exp)
     if not np.array_equal(np.asarray(got_cnt), np.asarray(exp_cnt)):
@@ -42,8 +74,8 @@ def compare_knn(got, got_cnt, exp, exp_cnt, P, Q, pos_of, k):
         return len(bad), 0
     dg = dist2(P, Q, got)
     de = dist2(P, Q, exp)
-    cg, dg = canonical_rows(got, dg, pos_of)
-    ce, de = canonical_rows(exp, de, pos_of)
+    cg, dg = canonical_rows(got, dg)
+    ce, de = canonical_rows(exp, de)
     same = (cg == ce).all(1)
     mism = 0
     ties = 0

@@ -2,8 +2,8 @@
 
 Everything goes through the public drop-in API, which calls the C ABI.  The
 expected answers come from the reference (golden fixtures) and from the CPU
-oracle, which follows the same (dist2, tree position) tie order as the GPU
-and therefore must agree bit for bit.
+oracle, which breaks distance ties by point index as the GPU does and
+therefore must agree bit for bit.
 """
 import math
 import os
@@ -22,12 +22,6 @@ def load(name):
     return dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
 
 
-def pos_of(rev, n):
-    p = np.full(n, -1, np.int64)
-    p[rev] = np.arange(len(rev))
-    return p
-
-
 @pytest.mark.parametrize("name", CASES)
 def test_build_is_the_reference_tree(gpu, name):
     g = load(name)
@@ -42,11 +36,10 @@ def test_queries_match_reference(gpu, name):
     g = load(name)
     P, Q, k = g["points"], g["queries"], int(g["k"])
     t = gpu.kdtree._build(P)
-    po = pos_of(g["reverse"], len(P))
     idx, cnt = gpu.kdtree.knn(t, Q, k)
-    assert compare_knn(idx, cnt, g["knn_idx"], g["knn_cnt"], P, Q, po, k)[0] == 0
+    assert compare_knn(idx, cnt, g["knn_idx"], g["knn_cnt"], P, Q, k)[0] == 0
     idx, cnt = gpu.kdtree.knn(t, Q, k, dmax=float(g["knn_r_dmax"]))
-    assert compare_knn(idx, cnt, g["knn_r_idx"], g["knn_r_cnt"], P, Q, po, k)[0] == 0
+    assert compare_knn(idx, cnt, g["knn_r_idx"], g["knn_r_cnt"], P, Q, k)[0] == 0
     rows = gpu.kdtree._query(t, Q, k=k)
     assert len(rows) == len(Q) and all(r.dtype == np.int32 for r in rows)
     assert all(np.array_equal(r, idx_row[:len(r)]) for r, idx_row in zip(rows, gpu.kdtree.knn(t, Q, k)[0]))
@@ -55,13 +48,95 @@ def test_queries_match_reference(gpu, name):
     assert np.array_equal(scnt, g["self_cnt"])
     ok = scnt > 0
     Qs = P[np.where(ok, sq, 0)]
-    assert compare_knn(sidx[ok], scnt[ok], g["self_idx"][ok], g["self_cnt"][ok], P, Qs[ok], po, k)[0] == 0
+    assert compare_knn(sidx[ok], scnt[ok], g["self_idx"][ok], g["self_cnt"][ok], P, Qs[ok], k)[0] == 0
     off, out = gpu.kdtree.rnear(t, Q, float(g["rnear_r"]))
     assert np.array_equal(off, g["rnear_off"]) and np.array_equal(out, g["rnear_idx"])
     off, out = gpu.kdtree.rnear(t, sq, float(g["rnear_r"]))
     assert np.array_equal(off, g["rself_off"]) and np.array_equal(out, g["rself_idx"])
     rows = gpu.kdtree._query(t, sq, k=None, dmax=float(g["rnear_r"]))
     assert np.array_equal(np.concatenate(rows), g["rself_idx"])
+
+
+def _tie_clouds():
+    """Inputs full of exact distance ties (as in tests/test_oracle.py)."""
+    import os as _os
+    g = lambda n: dict(np.load(_os.path.join(GOLDEN, f"{n}.npz")))["points"]  # noqa: E731
+    rng = np.random.default_rng(12)
+    return {
+        "f32_grid": g("f32_grid"),
+        "f32_nan_dups": g("f32_nan_dups"),
+        "identical": np.full((300, 3), 0.25, np.float32),
+        "int16_grid": rng.integers(0, 6, (3000, 3)).astype(np.int16),
+        "f64_lattice": np.stack(np.meshgrid(*[np.arange(10.0)] * 3), -1).reshape(-1, 3) * 0.5,
+    }
+
+
+@pytest.mark.parametrize("case", list(_tie_clouds()))
+def test_knn_ties_broken_by_point_index(gpu, port, case):
+    # at every exact distance tie the result is the k smallest
+    # (dist2, point index) pairs, identical to the oracle: point, self and
+    # all-points queries, every top-k capacity class and the device heaps
+    # (k > 64), with packet walks and per-lane walks
+    from pptk_b200 import _native as N
+    P = _tie_clouds()[case]
+    t = gpu.kdtree._build(P)
+    o = port.PortTree(P)
+    rng = np.random.default_rng(14)
+    qf = np.float64 if P.dtype == np.float64 else np.float32
+    sel = np.sort(rng.choice(len(P), min(len(P), 400), replace=False)).astype(np.int32)
+    Q = P[sel].astype(qf)
+    Q = Q[np.isfinite(Q.astype(np.float64)).all(1)]
+    allq = np.arange(t.n_valid, dtype=np.int32)
+    default = N.tune_get("lane_span")
+    try:
+        for span in (-1, 0):
+            N.tune_set("lane_span", span)
+            for k in (1, 4, 7, 16, 33, 64, 100):
+                gi, gc = gpu.kdtree.knn(t, Q, k)
+                oi, oc = o.knn(Q, k)
+                assert np.array_equal(gc, oc) and np.array_equal(gi, oi), (span, k, "points")
+                gi, gc = gpu.kdtree.knn(t, sel, k)
+                oi, oc = o.knn_self(sel, k)
+                assert np.array_equal(gc, oc) and np.array_equal(gi, oi), (span, k, "self")
+                gi, gc = gpu.kdtree.knn(t, None, k)
+                oi, oc = o.knn_self(allq, k)
+                assert np.array_equal(gc, oc) and np.array_equal(gi, oi), (span, k, "all")
+            gi, gc = gpu.kdtree.knn(t, Q, 16, dmax=1.0)
+            oi, oc = o.knn(Q, 16, dmax=1.0)
+            assert np.array_equal(gc, oc) and np.array_equal(gi, oi), (span, "dmax")
+    finally:
+        N.tune_set("lane_span", default)
+
+
+def test_forest_and_multi_tree_ties_broken_by_point_index(gpu, port):
+    # the same rule in ragged batches (one launch over many clouds) and in
+    # multi-tree batches (one launch over several resident trees)
+    import ctypes
+    from pptk_b200 import _native as N
+    from pptk_b200 import ragged
+    rng = np.random.default_rng(15)
+    clouds = [rng.integers(0, 5, (int(s), 3)).astype(np.float32) for s in (700, 40, 2500, 1, 900)]
+    off = np.concatenate([[0], np.cumsum([len(c) for c in clouds])])
+    f = ragged.Forest(np.concatenate(clouds), off)
+    for k in (5, 16, 40):
+        idx, cnt = f.knn(k)
+        for c, cl in enumerate(clouds):
+            oi, oc = port.PortTree(cl).knn_self(np.arange(len(cl), dtype=np.int32), k)
+            gi = np.where(idx[off[c]:off[c + 1]] >= 0, idx[off[c]:off[c + 1]] - off[c], -1)
+            assert np.array_equal(cnt[off[c]:off[c + 1]], oc) and np.array_equal(gi, oi), (k, c)
+    trees = [gpu.kdtree._build(c) for c in clouds]
+    qs = [c[rng.integers(0, len(c), min(len(c), 300))] + np.float32(0.5) for c in clouds]
+    rows = np.concatenate([[0], np.cumsum([len(q) for q in qs])]).astype(np.int64)
+    Q = np.ascontiguousarray(np.concatenate(qs))
+    handles = (ctypes.c_void_p * len(trees))(*[t._h.value for t in trees])
+    for k in (6, 20):
+        idx = np.empty((len(Q), k), np.int32)
+        cnt = np.empty(len(Q), np.int32)
+        N.call("pptkg_multi_knn", handles, len(trees), N.ptr(Q), N.ptr(rows), 0, N.MEM_HOST, k, float("inf"),
+               N.ptr(idx), N.ptr(cnt), None)
+        for g, (cl, q) in enumerate(zip(clouds, qs)):
+            oi, oc = port.PortTree(cl).knn(q, k)
+            assert np.array_equal(idx[rows[g]:rows[g + 1]], oi) and np.array_equal(cnt[rows[g]:rows[g + 1]], oc)
 
 
 @pytest.mark.parametrize("seed,dtype", [(0, np.float32), (1, np.float64)])

@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from _util import compare_knn
+from _util import brute_knn, compare_knn
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CASES = ["f32_uniform", "f64_uniform", "f32_nan_dups", "f32_grid", "f64_aniso"]
@@ -33,14 +33,11 @@ def test_port_queries_match_reference_golden(port, name):
     g = load(name)
     P, Q, k = g["points"], g["queries"], int(g["k"])
     t = port.PortTree(P)
-    rev = t.reverse_indices()
-    pos_of = np.full(len(P), -1, np.int64)
-    pos_of[rev] = np.arange(len(rev))
     idx, cnt = t.knn(Q, k)
-    mism, ties = compare_knn(idx, cnt, g["knn_idx"], g["knn_cnt"], P, Q, pos_of, k)
+    mism, ties = compare_knn(idx, cnt, g["knn_idx"], g["knn_cnt"], P, Q, k)
     assert mism == 0
     idx, cnt = t.knn(Q, k, dmax=float(g["knn_r_dmax"]))
-    mism, _ = compare_knn(idx, cnt, g["knn_r_idx"], g["knn_r_cnt"], P, Q, pos_of, k)
+    mism, _ = compare_knn(idx, cnt, g["knn_r_idx"], g["knn_r_cnt"], P, Q, k)
     assert mism == 0
     # self queries: the query point is removed from its own result
     sq = g["self_q"]
@@ -48,13 +45,47 @@ def test_port_queries_match_reference_golden(port, name):
     assert np.array_equal(scnt, g["self_cnt"])
     ok = scnt > 0
     Qs = np.where(ok[:, None], P[np.where(ok, sq, 0)], 0).astype(P.dtype)
-    mism, _ = compare_knn(sidx[ok], scnt[ok], g["self_idx"][ok], g["self_cnt"][ok], P, Qs[ok], pos_of, k)
+    mism, _ = compare_knn(sidx[ok], scnt[ok], g["self_idx"][ok], g["self_cnt"][ok], P, Qs[ok], k)
     assert mism == 0
     # r-near comes back in the reference's exact order
     off, out = t.rnear(Q, float(g["rnear_r"]))
     assert np.array_equal(off, g["rnear_off"]) and np.array_equal(out, g["rnear_idx"])
     off, out = t.rnear_self(sq, float(g["rnear_r"]))
     assert np.array_equal(off, g["rself_off"]) and np.array_equal(out, g["rself_idx"])
+
+
+def _tie_clouds():
+    """Inputs full of exact distance ties: the golden grid and duplicate
+    sets, all-identical points, and integer grids."""
+    rng = np.random.default_rng(12)
+    yield "f32_grid", load("f32_grid")["points"]
+    yield "f32_nan_dups", load("f32_nan_dups")["points"]
+    yield "identical", np.full((300, 3), 0.25, np.float32)
+    yield "int16_grid", rng.integers(0, 6, (3000, 3)).astype(np.int16)
+    yield "uint8_grid2d", rng.integers(0, 9, (2500, 2)).astype(np.uint8)
+    yield "f64_lattice", (np.stack(np.meshgrid(*[np.arange(10.0)] * 3), -1).reshape(-1, 3) * 0.5)
+
+
+@pytest.mark.parametrize("case", [c for c, _ in _tie_clouds()])
+def test_port_knn_breaks_ties_by_point_index(port, case):
+    # the specified kNN answer: the k smallest (dist2, point index) pairs.
+    # Exhaustive search defines it independently of any tree.
+    P = dict(_tie_clouds())[case]
+    t = port.PortTree(P)
+    rng = np.random.default_rng(13)
+    qf = np.float64 if P.dtype == np.float64 else np.float32
+    sel = rng.choice(len(P), min(len(P), 150), replace=False)
+    Q = P[sel].astype(qf)
+    finite = np.isfinite(Q.astype(np.float64)).all(1)
+    Q = Q[finite]
+    for k, dmax in ((1, np.inf), (7, np.inf), (16, np.inf), (16, 1.0)):
+        idx, cnt = t.knn(Q, k, dmax=dmax)
+        bi, bc = brute_knn(P, Q, k, dmax)
+        assert np.array_equal(cnt, bc) and np.array_equal(idx, bi), (case, k, dmax)
+        sq = sel[finite].astype(np.int32)
+        sidx, scnt = t.knn_self(sq, k, dmax=dmax)
+        bi, bc = brute_knn(P, Q, k, dmax, exclude=sq)
+        assert np.array_equal(scnt, bc) and np.array_equal(sidx, bi), (case, k, dmax)
 
 
 def test_knearest_known_answer(port):
@@ -166,3 +197,9 @@ def test_port_matches_reference_live(ref, dtype, dim):
     oa = a.rnear(q, 3.0)
     ob = b.rnear(q, 3.0)
     assert np.array_equal(oa[0], ob[0]) and np.array_equal(oa[1], ob[1])
+    # kNN: the same answers up to the reference's choice among tied points
+    # (integer clouds are full of ties)
+    qq = q.astype(np.float32) if np.dtype(dtype).kind != "f" else q
+    ia, ca = a.knn(q, 9)
+    ib, cb = b.knn(q, 9)
+    assert compare_knn(ia, ca, ib, cb, P, qq, 9)[0] == 0
