@@ -27,8 +27,12 @@ the whole stream (40M queries).
   per query) over its measured time inside the step, against the measured
   HBM copy bandwidth.
 * ``cpu_baseline``: the reference's own k-d tree (compiled from its sources
-  in oracle/_ref) with the restated normal loop, on a bounded sample, using
-  every host core.
+  in oracle/_ref), built once over the same 20M-point scene (serial build,
+  reported separately as ``build_s``), answering a bounded random sample of
+  the same request stream's rows -- kNN k=16 point queries and normal
+  queries (the restated normal loop over the resident tree) -- using every
+  host core.  Units are the serving form's: one query is one kNN request
+  row or one normal request row.
 * ``precision``: angular error (p50/p99/max, radians) of the FP32 normal
   path against FP64 on three clouds (200k uniform float32 k=16, the 20M
   scene k=16, 10M float64 planar patches offset 1e5 m k=24): all rows
@@ -37,9 +41,15 @@ the whole stream (40M queries).
 
 ``--workload plain`` times one drop-in ``estimate_normals`` over all 20M
 points instead (device build + fused kNN+PCA).  ``--impl reference`` times
-only the CPU reference path on the same metric.  Multi-GPU (torchrun):
-every rank runs an independent replica (weak scaling); there is no
-collective on the data path.
+only the CPU reference path on the same metric, config and units.
+Multi-GPU (torchrun): every rank runs an independent replica (weak
+scaling); there is no collective on the data path.
+
+With one GPU the default run also measures the other configurations
+briefly (``configs``: the scene's kNN k=32 and r-near r=0.5 m, the 4,096-
+cloud ragged batch, the 64-tree serving mix) with 3 warm-up and at most 5
+timed steps each.  Bulky per-stage data is printed on ``{"detail": ...}``
+lines before the final JSON line, which keeps the figures that are judged.
 """
 import argparse
 import ctypes
@@ -70,11 +80,16 @@ def parse():
     p.add_argument("--k", type=int, default=16)
     p.add_argument("--slots", type=int, default=3)
     p.add_argument("--max-batch", type=int, default=20_000_000, help="queries folded into one server batch")
+    p.add_argument("--batch-ms", type=float, default=None,
+                   help="time budget of one server batch (None: batches capped by --max-batch only)")
     p.add_argument("--max-host-batch", type=int, default=8_000_000,
                    help="queries folded into one server batch that returns numpy results")
     p.add_argument("--plain-sample", type=int, default=24, help="requests timed through the plain calls")
     p.add_argument("--latency-seconds", type=float, default=3.0)
-    p.add_argument("--cpu-sample", type=int, default=1_000_000)
+    p.add_argument("--cpu-sample", type=int, default=1_000_000,
+                   help="request rows (half kNN, half normals) per timed CPU-reference sample")
+    p.add_argument("--configs", default="scene,ragged,multitree",
+                   help="other configurations measured after the default workload (1 GPU; '' for none)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 angular error report")
@@ -172,6 +187,8 @@ def cpu_reference(points, k, sample, seed=0):
 
 
 def cpu_baseline_obj(pts, args):
+    """CPU baseline of the plain workload: the reference's per-call
+    estimate_normals (tree build included) on a sample of the scene."""
     try:
         qps, threads, dt, kind, ns = cpu_reference(pts, args.k, args.cpu_sample)
         return {"value": qps, "unit": "queries/s", "cores": threads, "kind": kind,
@@ -182,29 +199,94 @@ def cpu_baseline_obj(pts, args):
                 "sample": f"unavailable: {e}"}
 
 
+class RefScene:
+    """The reference's own k-d tree (oracle/_ref) built once over the whole
+    scene -- the resident-tree counterpart of the serving form.  The build is
+    the reference's serial RecursiveBuildHelper (TBB absent), timed and
+    reported on its own; queries run on every host thread."""
+
+    def __init__(self, pts):
+        from oracle import build_oracle
+        from oracle import oracle as O
+        if not O.ref_available():
+            build_oracle.build_ref()
+        self.pts = pts
+        t0 = time.perf_counter()
+        self.tree = O.RefTree(pts)
+        self.build_s = time.perf_counter() - t0
+        self.threads = O.ref_lib().ref_max_threads()
+
+    def mix_sample(self, mix, k, sample, seed):
+        """Answers `sample` rows drawn from the request stream (half from the
+        kNN requests' rows, as point queries; half from the normal requests'
+        rows); returns the timing of the queries alone."""
+        rng = np.random.default_rng(seed)
+        knn_rows = np.concatenate([r for kind, r in mix if kind == "knn"])
+        norm_rows = np.concatenate([r for kind, r in mix if kind == "normals"])
+        kq = knn_rows[rng.integers(0, len(knn_rows), sample // 2)]
+        nq = norm_rows[rng.integers(0, len(norm_rows), sample - sample // 2)]
+        Q = np.ascontiguousarray(self.pts[kq])
+        t0 = time.perf_counter()
+        self.tree.knn(Q, k)
+        t1 = time.perf_counter()
+        self.tree.normals(nq, k)
+        t2 = time.perf_counter()
+        return {"queries": len(kq) + len(nq), "seconds": t2 - t0, "value": (len(kq) + len(nq)) / (t2 - t0),
+                "knn_queries_per_s": len(kq) / (t1 - t0), "normal_queries_per_s": len(nq) / (t2 - t1)}
+
+    def describe(self, sample, k):
+        return (f"reference k-d tree over the whole scene ({len(self.pts)} points, built once: {self.build_s:.1f} s "
+                f"serial) answering {sample} random rows of the request stream per step ({sample // 2} kNN k={k} "
+                f"point queries + {sample - sample // 2} normal k={k} queries: kNN with the query point + "
+                "covariance + Jacobi eigensolve); TBB absent: OpenMP over the reference's per-query calls")
+
+
+def serving_cpu_baseline(pts, mix, args):
+    try:
+        ref = RefScene(pts)
+        r = ref.mix_sample(mix, args.k, args.cpu_sample, seed=0)
+        return {"value": r["value"], "unit": "queries/s", "cores": ref.threads, "kind": "reference",
+                "sample": ref.describe(args.cpu_sample, args.k), "build_s": ref.build_s,
+                "knn_queries_per_s": r["knn_queries_per_s"], "normal_queries_per_s": r["normal_queries_per_s"]}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": "queries/s", "cores": None, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+
+
 def run_reference(args):
+    """The reference arm, on the default workload's metric, units and config:
+    the reference tree resident over the 20M-point scene, each step a fresh
+    bounded sample of the same request stream."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
     from pptk_b200 import synth
     pts = synth.lidar_scene(args.points, seed=2)
+    mix = synth.request_mix(len(pts), len(pts), seed=11)
+    ref = RefScene(pts)
     vals = []
     for i in range(args.warmup + args.steps):
-        qps, threads, dt, kind, n = cpu_reference(pts, args.k, args.cpu_sample, seed=i)
+        r = ref.mix_sample(mix, args.k, args.cpu_sample, seed=100 + i)
         if i >= args.warmup:
-            vals.append((qps, dt))
-    value = float(np.mean([v[0] for v in vals]))
-    ms = float(np.mean([v[1] for v in vals])) * 1e3
-    sample = (f"{n} points drawn without replacement from the {args.points}-point scene each step; tree build + "
-              f"kNN k={args.k} + covariance + Jacobi eigensolve per point ({kind}; TBB absent: OpenMP over the "
-              f"reference's per-query calls)")
+            vals.append(r)
+    value = float(sum(v["queries"] for v in vals) / sum(v["seconds"] for v in vals))
+    ms = float(np.mean([v["seconds"] for v in vals])) * 1e3
+    knn_rate = float(np.mean([v["knn_queries_per_s"] for v in vals]))
+    norm_rate = float(np.mean([v["normal_queries_per_s"] for v in vals]))
     line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"lidar_scene_{args.points}_f32 kNN + normals k={args.k} r=inf (sampled)",
-                       "points": args.points, "k": args.k},
+            "config": {"workload": f"lidar_scene_{len(pts)}_f32 resident tree; rows of the kNN k={args.k} / normal "
+                                   f"k={args.k} request stream (sampled {args.cpu_sample} per step)",
+                       "points": len(pts), "k": args.k, "unit": "one kNN request row or one normal request row"},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": ref.threads, "kind": "reference",
+                             "sample": ref.describe(args.cpu_sample, args.k)},
+            "build_s": ref.build_s, "knn_queries_per_s": knn_rate, "normal_queries_per_s": norm_rate,
+            "plain_estimate_normals_call_s": {
+                "what": "one estimate_normals call over all scene points, as the reference API does it: serial "
+                        "build + the normal loop",
+                "seconds": ref.build_s + len(pts) / norm_rate},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -281,11 +363,12 @@ def device_timed(ctx, fn, steps):
     return e0.elapsed_time(e1) / steps, int(launches), clocks.stop()
 
 
-# DRAM bytes per query of k_normals (k=16, float32) measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's queries):
-# tree-order queries (profiles/k_normals_plain_lidar8M.md) and scattered
-# serving queries (profiles/k_normals_k_knn_serving_lidar8M.md); the bench's
-# per-launch traffic is this figure times the queries of a launch.
+# DRAM bytes per query of k_normals (k=16, float32) from one ncu capture each
+# (dram__bytes_read.sum + dram__bytes_write.sum of a launch over its
+# queries) on an 8M-point scene: tree-order queries and scattered serving
+# queries.  A scaling constant: the full-size launches are too large to
+# capture, and the traffic of a launch grows with the queries it answers,
+# so the reported traffic is this figure times the queries of a launch.
 TRAFFIC_PER_QUERY = {"tree_order": 126.8, "scattered": 160.5}
 
 
@@ -302,8 +385,7 @@ def roofline(ctx, stage_name, queries, traffic_kind):
             "traffic": traffic, "kernel": "k_normals (fused kNN+PCA)", "peak_kind": f"{peak_kind} hbm_gbs",
             "launches": cnt, "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch,
             "traffic_source": f"ncu DRAM bytes per query ({traffic_kind} queries, 8M-point capture) x queries "
-                              "per launch",
-            "limiter": "instruction issue (ALU pipe ~70 % busy, DRAM < 1.1 % of peak in the ncu captures)"}
+                              "per launch"}
 
 
 BUILD_STAGES = ("build", "build.prep", "build.attempt", "build.levels", "build.subtree", "build.finish",
@@ -690,7 +772,7 @@ def run_serving_workload(args, ctx):
 
     warm_dev, mix_dev = device_requests(warm_mix), device_requests(mix)
     srv = serving.Server(budget_bytes=150e9, slots=args.slots, max_batch_queries=args.max_batch,
-                         max_host_batch_queries=args.max_host_batch)
+                         max_host_batch_queries=args.max_host_batch, batch_ms=args.batch_ms)
     tid = srv.build(dev).result()
 
     def submit(reqs):
@@ -807,14 +889,16 @@ def run_serving_workload(args, ctx):
         e2e = {"value": ctx.world * per_step / dt, "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
     srv.close()
-    cpu = cpu_baseline_obj(pts, args) if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline else None
+    cpu = (serving_cpu_baseline(pts, mix, args)
+           if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline else None)
     return {"value": value, "ms_per_step": ms_max,
             "config": {"workload": f"lidar_scene_{n}_f32 resident tree; request stream of {len(mix)} requests "
                                    f"({n_knn} kNN k={k} point queries + {n_norm} normal k={k} r=inf queries, "
                                    "sizes log-uniform in [1k, 1M]) answered by the continuous-batching server",
                        "points": n, "k": k, "requests_per_step": len(mix), "queries_per_step": per_step,
-                       "slots": args.slots, "max_batch_queries": args.max_batch,
+                       "slots": args.slots, "max_batch_queries": args.max_batch, "batch_ms": args.batch_ms,
                        "l2": "scene (240 MB) and request inputs larger than L2 (126 MB); no flush",
+                       "unit": "one kNN request row or one normal request row",
                        "parallelism": f"replicas x{ctx.world}"},
             "plain": plain, "latency": latency, "latency_at_quarter_load": latency_q,
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof, "cpu_baseline": cpu,
@@ -874,6 +958,73 @@ def precision_report():
     return out
 
 
+WORKLOADS = {"serving": run_serving_workload, "plain": run_plain_workload, "ragged": run_ragged_workload,
+             "multitree": run_multitree_workload, "scene": run_scene_workload}
+
+# keys of a workload's result that go to the detail lines (bulky, not judged)
+DETAIL_KEYS = ("stages_ms", "autotune", "precision", "rnear", "build", "graph_replay", "steps_note")
+
+
+def _lat(d):
+    """p50/p99 of a latency block, compact."""
+    if not d:
+        return None
+    s = d.get("serving", d)
+    return {"offered_queries_per_s": d.get("offered_queries_per_s"), "p50_ms": s.get("p50_ms"),
+            "p99_ms": s.get("p99_ms"), "requests": s.get("requests")}
+
+
+def _precision_summary(prec):
+    return {name: {"p99_rad": v["vs_cpu_fp64_oracle_sample"]["p99"], "max_rad": v["vs_cpu_fp64_oracle_sample"]["max"],
+                   "p99_all_rows_vs_device_fp64_rad": v["vs_device_fp64_all_rows"]["p99"]}
+            for name, v in prec.items()}
+
+
+def compact_serving(res):
+    """The main figures of the serving workload, in a few hundred bytes."""
+    plain = res.get("plain") or {}
+    out = {"plain": {"value": plain.get("value"), "unit": "queries/s",
+                     "p50_ms": (plain.get("latency") or {}).get("p50_ms"),
+                     "p99_ms": (plain.get("latency") or {}).get("p99_ms"),
+                     "e2e_value": (plain.get("e2e") or {}).get("value")},
+           "latency": _lat(res.get("latency")), "latency_at_quarter_load": _lat(res.get("latency_at_quarter_load"))}
+    if plain.get("value"):
+        out["serving_over_plain"] = res["value"] / plain["value"]
+    return out
+
+
+def run_config(name, args, ctx):
+    """One other configuration, briefly (3 warm-up, <= 5 timed steps), as a
+    compact summary plus its full result for the detail lines."""
+    a = argparse.Namespace(**vars(args))
+    a.steps, a.warmup = max(1, min(args.steps, 5)), 3
+    a.no_cpu_baseline, a.no_e2e, a.latency_seconds = True, True, 2.0
+    if name == "ragged":
+        a.no_e2e = False
+    res = WORKLOADS[name](a, ctx)
+    summary = {"value": res["value"], "unit": "queries/s" if name != "ragged" else "points/s",
+               "ms_per_step": res["ms_per_step"], "steps": a.steps, "warmup": a.warmup,
+               "workload": res["config"]["workload"]}
+    if name == "scene":
+        rn = res["rnear"]
+        summary["rnear_r0.5"] = {"count_all_points_ms": rn["count_all_points_ms"],
+                                 "total_hits": rn["total_hits_all_points"],
+                                 "sample_count_and_fill_ms": rn["sample_count_and_fill_ms"],
+                                 "sample_queries": rn["sample_queries"]}
+    elif name == "ragged":
+        st = res["stages_ms"]
+        summary["stage_ms_per_step"] = {k: round(v["ms_per_step"], 2) for k, v in st.items()
+                                        if k in ("build", "forest.knn", "forest.normals")}
+        summary["graph_replay_queries_ms"] = res["graph_replay"]["ms_per_step"]
+        summary["e2e"] = res["e2e"]
+    elif name == "multitree":
+        summary["latency_quarter_load"] = _lat(res["latency"])
+        summary["latency_half_load"] = _lat(res["latency_at_half_load"])
+        summary["build_points_per_s"] = res["build"]["points_per_s"]
+    summary["clocks"] = res.get("clocks")
+    return summary, res
+
+
 def run_ours(args):
     ctx = Ctx()
     tuned = {}
@@ -883,17 +1034,36 @@ def run_ours(args):
         tuned[name] = int(val)
     ctx.lib.pptkg_profile_enable.argtypes = [ctypes.c_int]
     ctx.lib.pptkg_launch_count.restype = ctypes.c_int64
-    res = {"serving": run_serving_workload, "plain": run_plain_workload,
-           "ragged": run_ragged_workload, "multitree": run_multitree_workload,
-           "scene": run_scene_workload}[args.workload](args, ctx)
-    if ctx.rank == 0 and ctx.world == 1 and not args.no_precision:
-        res["precision"] = precision_report()
+    res = WORKLOADS[args.workload](args, ctx)
+    details = {}
+    one = ctx.rank == 0 and ctx.world == 1
+    if one and not args.no_precision:
+        details["precision"] = precision_report()
+    configs = {}
+    if one and args.workload == "serving" and args.configs:
+        for name in [c for c in args.configs.split(",") if c]:
+            summary, full = run_config(name, args, ctx)
+            configs[name] = summary
+            details[f"config.{name}"] = full
     if ctx.rank == 0:
+        for key in DETAIL_KEYS:
+            if key in res:
+                details[key] = res.pop(key)
+        if args.workload == "serving":
+            details["plain"] = res.get("plain")
+            details["latency"] = {"half_load": res.get("latency"), "quarter_load": res.get("latency_at_quarter_load")}
+            res.update(compact_serving(res))
+        for name, d in details.items():
+            print(json.dumps({"detail": name, "data": d}, default=str), flush=True)
         line = {"metric": METRIC, "value": res.pop("value"), "unit": "queries/s", "n_gpus": ctx.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic"}
         line.update(res)
+        if "precision" in details:
+            line["precision_fp32_vs_fp64_oracle"] = _precision_summary(details["precision"])
+        if configs:
+            line["configs"] = configs
         if tuned:
             line["config"]["tune"] = tuned
         print(json.dumps(line), flush=True)

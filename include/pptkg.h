@@ -158,13 +158,19 @@ PPTKG_API int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices,
  * the device) is not acceptable.  The caller passes device pointers for the
  * query rows (indices, or NULL for rows 0..m-1; m = 0 with NULL means all
  * rows) and for the outputs, as in pptkg_tree_normals with PPTKG_MEM_DEVICE.
+ * A pointer that is not device (or managed) memory of the tree's device is
+ * rejected with PPTKG_E_INVALID before anything reads it.
  * Limits: m <= PPTKG_NOALLOC_MAX_QUERIES (65536), 1 <= k <= 16; larger sizes
  * are rejected with PPTKG_E_INVALID.  The scratch (about 4.7 MB) is a static
  * device array held by every GPU that loads the library until the process
  * exits; the first call on a device looks up its address, so make that first
- * call before any stream capture.  All calls share that one array: calls that
- * overlap on the GPU (other streams, other host threads) race and must be
- * serialized by the caller.  No memory is allocated or freed. */
+ * call before any stream capture.  The address is kept for the rest of the
+ * process, like every device pointer the library holds: a cudaDeviceReset
+ * invalidates it together with the trees.  Each call waits for its stream at
+ * the end, to read the status word of the kernels' checks.  All calls share
+ * that one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialized by the caller.  No memory is
+ * allocated or freed. */
 #define PPTKG_NOALLOC_MAX_QUERIES 65536
 #define PPTKG_NOALLOC_MAX_K 16
 PPTKG_API int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* indices, int64_t m, int k, float r,

@@ -59,6 +59,7 @@ def _bind(lib, prefix):
         sig["knn"] = (None, [_vp, _vp, _i64, _i32, _i32, _dbl, _vp, _vp, _i32])
         sig["estimate_normals"] = (None, [_vp, _i64, _i32, _i32, _flt, _vp, _i64, _i32, _vp, _vp, _vp, _i32,
                                           _vp])
+        sig["tree_normals"] = (None, [_vp, _vp, _vp, _i64, _i32, _flt, _i32, _vp, _vp, _vp, _i32])
     sig["max_threads"] = (_i32, [])
     for name, (res, args) in sig.items():
         fn = getattr(lib, f"{prefix}_{name}")
@@ -173,6 +174,19 @@ class RefTree(_Tree):
         cnt = np.empty(m, np.int32)
         self._fn("knn")(self._h, _ptr(q), m, DTYPES[q.dtype], k, float(dmax), _ptr(idx), _ptr(cnt), nthreads)
         return idx, cnt
+
+    def normals(self, rows, k, r=np.inf, nthreads=0):
+        """The restated normal loop over this (resident) tree for the given
+        rows of its input: (normals m x 3, sizes m)."""
+        if self.dim != 3 or self.dtype not in (np.float32, np.float64):
+            raise TypeError("normals need a 3-d float32/float64 tree")
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        m = len(rows)
+        ev = np.empty((m, 3), self.dtype)
+        sz = np.empty(m, np.int32)
+        self._fn("tree_normals")(self._h, _ptr(self.points), _ptr(rows), m, int(k), float(r), 1, _ptr(ev), None,
+                                 _ptr(sz), nthreads)
+        return ev, sz
 
 
 _port = None

@@ -288,6 +288,67 @@ void ref_estimate_normals(const void* pts, int64_t n, int dtype, int k, float r,
     run(double());
 }
 
+// The normal loop of ref_estimate_normals (estimate_normals.cpp:64-110) over
+// an already built reference tree `hp` (float32/float64, dim 3) whose input
+// array was `pts` (n x 3, original order): the resident-tree form, so that
+// a timed run holds queries only.  sub: m query rows (original indices).
+void ref_tree_normals(void* hp, const void* pts, const int32_t* sub, int64_t m, int k, float r, int num_eigen,
+                      void* evecs, void* evals, int32_t* sizes, int nthreads) {
+  Handle* h = (Handle*)hp;
+  auto run = [&](auto t) {
+    typedef decltype(t) T;
+    const pointkd::KdTree<T, 3>& tree = *(const pointkd::KdTree<T, 3>*)h->tree;
+    const T* P = (const T*)pts;
+    const T d_max = (T)r;
+    T* ev = (T*)evecs;
+    T* ew = (T*)evals;
+#pragma omp parallel for schedule(static, 1000) num_threads(threads_or_max(nthreads))
+    for (int64_t i = 0; i < m; i++) {
+      pointkd::Indices idx;
+      const T* q = P + (int64_t)sub[i] * 3;
+      if (k == -1)
+        tree.RNearNeighbors(idx, q, d_max);
+      else
+        tree.KNearestNeighbors(idx, q, k, d_max);
+      size_t cnt = idx.size();
+      T mean[3] = {0, 0, 0};
+      for (size_t j = 0; j < cnt; j++)
+        for (int c = 0; c < 3; c++) mean[c] += P[(int64_t)idx[j] * 3 + c];
+      for (int c = 0; c < 3; c++) mean[c] /= (T)cnt;
+      T C[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (size_t j = 0; j < cnt; j++) {
+        T x[3];
+        for (int c = 0; c < 3; c++) x[c] = P[(int64_t)idx[j] * 3 + c] - mean[c];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) C[a * 3 + b] += x[a] * x[b];
+      }
+      for (int a = 0; a < 9; a++) C[a] /= (T)cnt;
+      T w[3], V[9];
+      oracle::jacobi3<T>(C, w, V);
+      if (ev) {
+        if (num_eigen == 1) {
+          for (int c = 0; c < 3; c++) ev[i * 3 + c] = V[c * 3 + 0];
+        } else {
+          for (int e = 0; e < 3; e++)
+            for (int c = 0; c < 3; c++) ev[i * 9 + e * 3 + c] = V[c * 3 + e];
+        }
+      }
+      if (ew) {
+        if (num_eigen == 1)
+          ew[i] = w[0];
+        else
+          for (int e = 0; e < 3; e++) ew[i * 3 + e] = w[e];
+      }
+      if (sizes) sizes[i] = (int32_t)cnt;
+    }
+  };
+  if (h->dim != 3) return;
+  if (h->dtype == oracle::F32)
+    run(float());
+  else if (h->dtype == oracle::F64)
+    run(double());
+}
+
 int ref_max_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -674,12 +674,33 @@ int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices, int64_t m
   });
 }
 
+// The allocation-free entry takes device memory only: a host pointer would be
+// read by the kernels as if it were a device address.  Rejects (without
+// touching the memory) anything that is not device or managed memory
+// reachable from the tree's device.
+static void require_device_memory(const void* p, int device, const char* what) {
+  if (!p) return;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw Error(E_INVALID, std::string(what) + ": not a pointer the CUDA runtime knows");
+  }
+  if (a.type == cudaMemoryTypeManaged) return;
+  if (a.type != cudaMemoryTypeDevice)
+    throw Error(E_INVALID, std::string(what) + " must point to device memory (host memory given)");
+  if (a.device != device) throw Error(E_INVALID, std::string(what) + " lies on another device than the tree");
+}
+
 int pptkg_tree_normals_noalloc(const pptkg_tree* tree, const int32_t* indices, int64_t m, int k, float r,
                                int num_eigen, int precision, void* out_evecs, void* out_evals, int32_t* out_sizes,
                                void* stream) {
   return guarded([&] {
     const TreeBase* t = tree_of(tree);
     DeviceGuard g(t->device);
+    require_device_memory(indices, t->device, "indices");
+    require_device_memory(out_evecs, t->device, "out_evecs");
+    require_device_memory(out_evals, t->device, "out_evals");
+    require_device_memory(out_sizes, t->device, "out_sizes");
     if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
     if (t->rec_dtype != F32 && t->rec_dtype != F64) throw Error(E_TYPE, "normals need float32 or float64 points");
     if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");

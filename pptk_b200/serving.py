@@ -47,7 +47,8 @@ def _first_k(idx, cnt, k, k_launch):
 
 
 class Request:
-    __slots__ = ("kind", "args", "future", "t_submit", "t_start", "t_done", "bytes", "m", "key")
+    __slots__ = ("kind", "args", "future", "t_submit", "t_start", "t_done", "bytes", "m", "key", "next_row",
+                 "rows_done", "parts")
 
     def __init__(self, kind, args, nbytes, m, key=None):
         self.kind = kind
@@ -145,7 +146,9 @@ class GpuEngine:
             ids = []
             for t, ix in zip(trees, indices):
                 if ix is None:
-                    ix = torch.arange(t.n, dtype=torch.int32, device=self.device)
+                    ix = RowRange(0, t.n)
+                if isinstance(ix, RowRange):
+                    ix = torch.arange(ix.lo, ix.hi, dtype=torch.int32, device=self.device)
                 ids.append(torch.as_tensor(ix, device=self.device).to(torch.int32))
             uniq, groups, rows, spans = self._merge(trees, ids)
             q = torch.cat([x for grp in groups for x in grp]).contiguous()
@@ -169,32 +172,103 @@ class GpuEngine:
     def synchronize(self, stream):
         stream.synchronize()
 
+    def mark(self, stream):
+        """A timing event recorded on `stream` at this point of its work."""
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+
+class _Slice:
+    """Rows [lo, hi) of a request, the unit that batches are made of."""
+    __slots__ = ("r", "lo", "hi")
+
+    def __init__(self, r, lo, hi):
+        self.r, self.lo, self.hi = r, lo, hi
+
+    @property
+    def m(self):
+        return self.hi - self.lo
+
+
+class RowRange:
+    """Rows lo .. hi-1 of a tree's input, standing for a normal request over
+    all rows (indices None) cut into slices."""
+    __slots__ = ("lo", "hi")
+
+    def __init__(self, lo, hi):
+        self.lo, self.hi = lo, hi
+
+    def __len__(self):
+        return self.hi - self.lo
+
+
+def _rows(x, lo, hi):
+    if isinstance(x, RowRange):
+        return RowRange(x.lo + lo, x.lo + hi)
+    return x[lo:hi]
+
+
+def _concat(parts):
+    """Joins the per-slice results of one request (numpy arrays or CUDA
+    tensors, or tuples of them) along the query rows."""
+    if len(parts) == 1:
+        return parts[0]
+    if isinstance(parts[0], tuple):
+        return tuple(_concat([p[i] for p in parts]) for i in range(len(parts[0])))
+    if isinstance(parts[0], np.ndarray):
+        return np.concatenate(parts)
+    import torch
+    return torch.cat(parts)
+
 
 class Server:
     """Continuous-batching server.
 
     budget_bytes: HBM the server may commit to resident trees plus the
         transient needs of admitted requests.
-    slots: batches that may run at once, each on its own CUDA stream; the
-        last `fast_slots` of them run on high-priority streams and take the
-        batches of at most `small_batch` queries first.
-    max_batch_queries: upper bound on the queries folded into one batch.
-    max_host_batch_queries: the same bound for batches that return numpy
+    slots: batches that may run at once, each on its own CUDA stream.  The
+        last `fast_slots` of them run on high-priority streams and serve
+        small requests only (at most `small_batch` queries each), so that a
+        small request never waits behind the rows of a large one.
+    batch_ms: time budget of one batch.  The queries folded into a batch are
+        capped at the measured rate (queries per second of recent batches)
+        times this budget, within [min_batch_queries, max_batch_queries];
+        a request larger than the cap is answered in slices of the cap, so
+        requests submitted after it interleave with its slices.
+    max_host_batch_queries: the upper bound for batches that return numpy
         results: smaller batches let one batch's host copies overlap another
         batch's kernels.
+
+    trace: keep, for every batch, CUDA events recorded on its stream before
+        and after its work (``trace`` list of (kinds, fast slot, start,
+        end)), so that the device-side overlap of batches can be checked.
+
+    Requests are admitted first-in first-out within each of two queues
+    (small requests, and everything else) against the HBM budget; a
+    request's Future may be cancelled (``future.cancel()``) until its last
+    rows are answered: rows not yet started are never run, and the answer of
+    rows in flight is discarded.  A batch that fails fails the requests it
+    held rows of; the server keeps serving.
     """
 
     def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=20_000_000, engine=None,
-                 fast_slots=1, small_batch=1_000_000, max_host_batch_queries=8_000_000):
+                 fast_slots=1, small_batch=1_000_000, max_host_batch_queries=8_000_000, batch_ms=None,
+                 min_batch_queries=1_000_000, trace=False):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)
         self.max_batch = int(max_batch_queries)
         self.max_host_batch = int(max_host_batch_queries)
         self.small_batch = int(small_batch)
+        self.batch_ms = None if batch_ms is None else float(batch_ms)
+        self.min_batch = int(min_batch_queries)
+        self._rate = None  # queries per second of recent batches (EMA)
+        self.trace = [] if trace else None
         self.trees = {}
         self.tree_bytes = {}
         self._next_id = 0
-        self._pending = deque()
+        self._small = deque()
+        self._large = deque()
         self._committed = 0.0
         self._cv = threading.Condition()
         fast_slots = max(0, min(int(fast_slots), slots - 1))
@@ -235,13 +309,22 @@ class Server:
         """Future of the normals (m x 3) of the tree's input rows `indices`
         (all rows when None), over k nearest neighbours within r.  to_host
         as for knn (default: when the indices are a numpy array)."""
-        m = self.trees[tree_id].n if indices is None else int(len(indices))
         host = isinstance(indices, np.ndarray) if to_host is None else bool(to_host)
+        if indices is None:
+            tree = self.trees.get(tree_id)
+            if tree is None:
+                f = Future()
+                f.set_exception(KeyError(f"unknown tree {tree_id}"))
+                return f
+            indices = RowRange(0, tree.n)
+        m = int(len(indices))
         req = Request("normals", (tree_id, indices), m * (QUERY_BYTES + 4 * int(k)), m,
                       key=("normals", int(k), float(r), precision, host))
         return self._submit(req)
 
     def rnear(self, tree_id, queries, dmax):
+        """Future of (offsets m + 1, hits) of the points within dmax of each
+        query point, in the reference's order."""
         m = int(queries.shape[0])
         return self._submit(Request("rnear", (tree_id, queries, float(dmax)), m * QUERY_BYTES * 8, m))
 
@@ -256,39 +339,73 @@ class Server:
         if r.bytes > self.budget:
             r.future.set_exception(MemoryError(f"request needs {r.bytes:.3g} B, above the budget {self.budget:.3g} B"))
             return r.future
+        r.next_row = 0
+        r.rows_done = 0
+        r.parts = {}
         with self._cv:
             if not self._running:
                 raise RuntimeError("server closed")
-            self._pending.append(r)
+            small = r.kind in ("knn", "normals", "rnear") and r.m <= self.small_batch
+            (self._small if small else self._large).append(r)
             self._cv.notify_all()
         return r.future
 
     # ----------------------------------------------------------- scheduler --
-    def _admit(self):
-        """FIFO admission under the budget.  A build or r-near request runs
-        as a batch of its own; consecutive kNN / normal requests are folded
-        into one batch up to max_batch_queries."""
+    def batch_cap(self, host=False):
+        """Queries a kNN / normal batch may hold now."""
+        top = min(self.max_host_batch, self.max_batch) if host else self.max_batch
+        if self.batch_ms is None or self._rate is None:
+            return top
+        return int(min(top, max(self.min_batch, self._rate * self.batch_ms / 1e3)))
+
+    def _admit(self, fast):
+        """Slices of requests for the next batch, first-in first-out within a
+        queue under the budget.  A fast slot takes small requests only, up to
+        small_batch queries; another slot takes the large queue first.  A
+        build or r-near request runs as a batch of its own; kNN and normal
+        rows are folded up to the batch cap, the last request possibly cut."""
+        queues = [self._small] if fast else [self._large, self._small]
+        for q in queues:
+            out = self._admit_from(q, self.small_batch if fast else None)
+            if out:
+                return out
+        return []
+
+    def _admit_from(self, q, limit):
         out = []
         queries = 0
         host = False
-        while self._pending:
-            r = self._pending[0]
+        while q:
+            r = q[0]
+            if r.future.done():  # cancelled (or failed) while queued: its rows
+                q.popleft()      # not yet admitted never run (nothing of them was committed)
+                continue
             if r.kind != "build" and r.args[0] not in self.trees:
-                self._pending.popleft()
+                q.popleft()
                 r.future.set_exception(KeyError(f"unknown tree {r.args[0]}"))
                 continue
             exclusive = r.kind in ("build", "rnear")
             r_host = bool(r.key and r.key[-1] is True)
-            cap = self.max_host_batch if (host or r_host) else self.max_batch
-            if out and (exclusive or queries + r.m > cap):
+            cap = self.batch_cap(host or r_host)
+            if limit is not None:
+                cap = min(cap, limit)
+            if out and (exclusive or queries >= cap):
                 break
-            if self._committed + r.bytes > self.budget:
+            take = r.m - r.next_row if exclusive else min(r.m - r.next_row, max(cap - queries, 0))
+            if take <= 0 and r.m > 0:
                 break
-            self._pending.popleft()
-            self._committed += r.bytes
-            out.append(r)
-            queries += r.m
+            part = r.bytes * take / max(r.m, 1) if r.m else r.bytes
+            if self._committed + part > self.budget:
+                break
+            if r.next_row == 0:
+                r.t_start = time.perf_counter()
+            out.append(_Slice(r, r.next_row, r.next_row + take))
+            r.next_row += take
+            self._committed += part
+            queries += take
             host = host or r_host
+            if r.next_row >= r.m:
+                q.popleft()
             if exclusive:
                 break
         return out
@@ -296,35 +413,40 @@ class Server:
     def _loop(self):
         while True:
             with self._cv:
-                while self._running and (not self._pending or not self._free):
+                while self._running and (not (self._small or self._large) or not self._free):
                     self._cv.wait(0.01)
-                if not self._running and not self._pending:
+                if not self._running and not (self._small or self._large):
                     return
                 if not self._free:
                     continue
-                batch = self._admit()
+                batch, slot = [], None
+                # a fast slot first when small requests wait, then the others
+                for i in sorted(range(len(self._free)), key=lambda j: not self._free[j][1]):
+                    batch = self._admit(self._free[i][1])
+                    if batch:
+                        slot = self._free.pop(i)
+                        break
                 if not batch:
                     self._cv.wait(0.001)
                     continue
-                small = sum(r.m for r in batch) <= self.small_batch
-                pick = next((i for i, (_, fast) in enumerate(self._free) if fast == small), len(self._free) - 1)
-                slot = self._free.pop(pick)
                 self._batches += 1
             self._pool.submit(self._run, batch, slot)
 
     def _run(self, batch, slot):
         stream = slot[0]
         t0 = time.perf_counter()
-        for r in batch:
-            r.t_start = t0
+        live = [s for s in batch if not s.r.future.done()]
+        marks = self.trace is not None and hasattr(self.engine, "mark")
         try:
+            e0 = self.engine.mark(stream) if marks else None
             groups = {}
-            for r in batch:
-                groups.setdefault(r.key if r.key else (r.kind, id(r)), []).append(r)
-            for key, rs in groups.items():
-                kind = rs[0].kind
+            for sl in live:
+                r = sl.r
+                groups.setdefault(r.key if r.key else (r.kind, id(r)), []).append(sl)
+            for key, ss in groups.items():
+                kind = ss[0].r.kind
                 if kind == "build":
-                    r = rs[0]
+                    r = ss[0].r
                     tree = self.engine.build(*r.args, stream)
                     with self._cv:
                         tid = self._next_id
@@ -332,41 +454,64 @@ class Server:
                         self.trees[tid] = tree
                         self.tree_bytes[tid] = r.m * TREE_BYTES_PER_POINT
                         self._committed += self.tree_bytes[tid]
-                    self._finish([r], [tid], stream)
+                    self._finish(ss, [tid], stream)
                 elif kind == "knn":
-                    trees = [self.trees[r.args[0]] for r in rs]
-                    kl = max(r.args[2] for r in rs)
-                    res = self.engine.knn_batch(trees, [r.args[1] for r in rs], kl, key[2], stream, host=key[4])
-                    res = [_first_k(i, c, r.args[2], kl) for (i, c), r in zip(res, rs)]
-                    self._finish(rs, res, stream)
+                    trees = [self.trees[s.r.args[0]] for s in ss]
+                    kl = max(s.r.args[2] for s in ss)
+                    res = self.engine.knn_batch(trees, [_rows(s.r.args[1], s.lo, s.hi) for s in ss], kl, key[2],
+                                                stream, host=key[4])
+                    res = [_first_k(i, c, s.r.args[2], kl) for (i, c), s in zip(res, ss)]
+                    self._finish(ss, res, stream)
                 elif kind == "normals":
-                    trees = [self.trees[r.args[0]] for r in rs]
-                    res = self.engine.normals_batch(trees, [r.args[1] for r in rs], key[1], key[2], key[3], stream,
-                                                    host=key[4])
-                    self._finish(rs, res, stream)
+                    trees = [self.trees[s.r.args[0]] for s in ss]
+                    res = self.engine.normals_batch(trees, [_rows(s.r.args[1], s.lo, s.hi) for s in ss], key[1],
+                                                    key[2], key[3], stream, host=key[4])
+                    self._finish(ss, res, stream)
                 elif kind == "rnear":
-                    r = rs[0]
+                    r = ss[0].r
                     res = self.engine.rnear(self.trees[r.args[0]], r.args[1], r.args[2], stream)
-                    self._finish([r], [res], stream)
+                    self._finish(ss, [res], stream)
+            if marks:
+                e1 = self.engine.mark(stream)
+                with self._cv:
+                    self.trace.append((sorted({s.r.kind for s in live}), slot[1], e0, e1))
+            q = sum(s.m for s in live if s.r.kind in ("knn", "normals"))
+            dt = time.perf_counter() - t0
+            if q >= self.min_batch // 4 and dt > 0:
+                with self._cv:
+                    self._rate = q / dt if self._rate is None else 0.7 * self._rate + 0.3 * (q / dt)
         except Exception as e:  # a failed batch fails its requests, not the server
-            for r in batch:
-                if not r.future.done():
-                    r.future.set_exception(e)
+            for sl in batch:
+                if not sl.r.future.done():
+                    sl.r.future.set_exception(e)
         finally:
             with self._cv:
-                for r in batch:
-                    self._committed -= r.bytes
+                for sl in batch:
+                    self._committed -= sl.r.bytes * sl.m / max(sl.r.m, 1) if sl.r.m else sl.r.bytes
                 self._free.append(slot)
                 self._cv.notify_all()
 
-    def _finish(self, rs, results, stream):
+    def _finish(self, slices, results, stream):
         self.engine.synchronize(stream)
         t = time.perf_counter()
-        for r, res in zip(rs, results):
+        for sl, res in zip(slices, results):
+            r = sl.r
+            with self._cv:
+                r.parts[sl.lo] = res
+                r.rows_done += sl.m
+                complete = r.rows_done >= r.m
+            if not complete:
+                continue
             r.t_done = t
+            out = _concat([r.parts[lo] for lo in sorted(r.parts)]) if r.kind in ("knn", "normals") else res
+            r.parts = {}
             with self._cv:
                 self._done.append((r.kind, r.m, r.t_submit, r.t_done))
-            r.future.set_result(res)
+            if not r.future.done():
+                try:
+                    r.future.set_result(out)
+                except Exception:  # cancelled meanwhile
+                    pass
 
     # --------------------------------------------------------------- info --
     def stats(self, since=0.0):
@@ -390,10 +535,11 @@ class Server:
         RuntimeError, running batches finish."""
         with self._cv:
             self._running = False
-            while self._pending:
-                r = self._pending.popleft()
-                if not r.future.done():
-                    r.future.set_exception(RuntimeError("server closed"))
+            for q in (self._small, self._large):
+                while q:
+                    r = q.popleft()
+                    if not r.future.done():
+                        r.future.set_exception(RuntimeError("server closed"))
             self._cv.notify_all()
         self._thread.join()
         self._pool.shutdown(wait=True)

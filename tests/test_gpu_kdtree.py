@@ -83,8 +83,10 @@ def test_knn_ties_broken_by_point_index(gpu, port, case):
     o = port.PortTree(P)
     rng = np.random.default_rng(14)
     qf = np.float64 if P.dtype == np.float64 else np.float32
-    sel = np.sort(rng.choice(len(P), min(len(P), 400), replace=False)).astype(np.int32)
-    Q = P[sel].astype(qf)
+    # index queries address rows 0 .. num_points()-1 (the valid count), as
+    # in the reference
+    sel = np.sort(rng.choice(t.n_valid, min(t.n_valid, 400), replace=False)).astype(np.int32)
+    Q = P[rng.choice(len(P), min(len(P), 400), replace=False)].astype(qf)
     Q = Q[np.isfinite(Q.astype(np.float64)).all(1)]
     allq = np.arange(t.n_valid, dtype=np.int32)
     default = N.tune_get("lane_span")

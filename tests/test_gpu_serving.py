@@ -2,6 +2,7 @@
 same alone and in the mix (bit for bit)."""
 import ctypes
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -59,49 +60,131 @@ def _np(x):
 
 
 def test_server_answers_are_the_same_alone_and_in_the_mix(gpu):
+    # kNN, normal, r-near and build requests of very different sizes, from
+    # four client threads at once, against the same requests one at a time
     import torch
     from pptk_b200 import serving
     rng = np.random.default_rng(3)
     clouds = [rng.random((int(s), 3), dtype=np.float32) for s in (80_000, 30_000, 150_000)]
-    srv = serving.Server(budget_bytes=8e9, slots=3)
+    srv = serving.Server(budget_bytes=8e9, slots=3, max_batch_queries=6_000, min_batch_queries=1_000,
+                         small_batch=2_000)
     ids = [f.result(timeout=120) for f in [srv.build(c) for c in clouds]]
     reqs = []
-    for i in range(40):
+    for i in range(48):
         g = int(rng.integers(0, 3))
-        if i % 2:
+        u = i % 6
+        if u in (1, 3):
             q = clouds[g][rng.integers(0, len(clouds[g]), int(rng.integers(1, 20_000)))] + np.float32(2e-3)
             reqs.append(("knn", g, q))
-        else:
+        elif u in (0, 2):
             ix = rng.integers(0, len(clouds[g]), int(rng.integers(1, 20_000))).astype(np.int32)
             reqs.append(("normals", g, ix))
+        elif u == 4:
+            q = clouds[g][rng.integers(0, len(clouds[g]), int(rng.integers(1, 3_000)))]
+            reqs.append(("rnear", g, q))
+        else:
+            reqs.append(("build", g, rng.random((int(rng.integers(1_000, 60_000)), 3), dtype=np.float32)))
     # every third request passes CUDA tensors (and gets CUDA tensors back)
     reqs = [(kind, g, torch.from_numpy(a).cuda() if j % 3 == 0 else a) for j, (kind, g, a) in enumerate(reqs)]
     results = [None] * len(reqs)
 
+    def submit(kind, g, a):
+        if kind == "knn":
+            return srv.knn(ids[g], a, k=8)
+        if kind == "normals":
+            return srv.normals(ids[g], a, k=8)
+        if kind == "rnear":
+            return srv.rnear(ids[g], a, 0.03)
+        return srv.build(a)
+
     def client(lo, hi):
         for j in range(lo, hi):
-            kind, g, a = reqs[j]
-            f = srv.knn(ids[g], a, k=8) if kind == "knn" else srv.normals(ids[g], a, k=8)
-            results[j] = f.result(timeout=120)
+            results[j] = submit(*reqs[j]).result(timeout=120)
 
-    threads = [threading.Thread(target=client, args=(j, j + 10)) for j in range(0, 40, 10)]
+    threads = [threading.Thread(target=client, args=(j, j + 12)) for j in range(0, 48, 12)]
     [t.start() for t in threads]
     [t.join() for t in threads]
     st = srv.stats()
-    assert st["knn"]["requests"] == 20 and st["normals"]["requests"] == 20
+    assert st["knn"]["requests"] == 16 and st["normals"]["requests"] == 16 and st["rnear"]["requests"] == 8
+    assert st["batches"] > 8
     # alone: the same requests one at a time
     for j, ((kind, g, a), got) in enumerate(zip(reqs, results)):
-        f = srv.knn(ids[g], a, k=8) if kind == "knn" else srv.normals(ids[g], a, k=8)
-        alone = f.result(timeout=120)
+        alone = submit(kind, g, a).result(timeout=120)
         on_device = j % 3 == 0
         if kind == "knn":
             assert all(torch.is_tensor(x) == on_device for x in got)
             assert np.array_equal(_np(got[0]), _np(alone[0])) and np.array_equal(_np(got[1]), _np(alone[1]))
             direct, _ = gpu.kdtree.knn(srv.trees[ids[g]], _np(a), 8)
             assert np.array_equal(_np(got[0]), direct)
-        else:
+        elif kind == "normals":
             assert torch.is_tensor(got) == on_device
             assert np.array_equal(_np(got), _np(alone))
+        elif kind == "rnear":
+            off, hits = gpu.kdtree.rnear(srv.trees[ids[g]], _np(a), 0.03)
+            for x in (got, alone):
+                assert np.array_equal(_np(x[0]), off) and np.array_equal(_np(x[1]), hits)
+        else:
+            # a tree built in the mix answers like a tree built alone
+            pts = _np(a)
+            q = pts[:500] + np.float32(1e-3)
+            direct, _ = gpu.kdtree.knn(gpu.kdtree._build(pts), q, 6)
+            for tid in (got, alone):
+                assert np.array_equal(srv.knn(tid, q, k=6).result(timeout=120)[0], direct)
+    srv.close()
+
+
+def test_server_batches_overlap_on_the_device(gpu):
+    # three slots, requests sliced into several batches: CUDA events on the
+    # slot streams show batches of different slots in flight on the device
+    # at the same time
+    import torch
+    from pptk_b200 import serving
+    rng = np.random.default_rng(9)
+    cloud = rng.random((1_000_000, 3), dtype=np.float32)
+    srv = serving.Server(budget_bytes=8e9, slots=3, max_batch_queries=400_000, min_batch_queries=100_000,
+                         small_batch=1, trace=True)
+    tid = srv.build(torch.from_numpy(cloud).cuda()).result(timeout=120)
+    torch.cuda.synchronize()
+    ref = torch.cuda.Event(enable_timing=True)
+    ref.record()  # before every batch event below
+    torch.cuda.synchronize()
+    futs = [srv.normals(tid, torch.from_numpy(rng.integers(0, len(cloud), 1_200_000).astype(np.int32)).cuda(),
+                        k=16) for _ in range(2)]
+    futs.append(srv.knn(tid, torch.from_numpy(cloud[:1_200_000 // 2]).cuda(), k=16))
+    [f.result(timeout=120) for f in futs]
+    torch.cuda.synchronize()
+    tr = [t for t in srv.trace if t[0] != ["build"]]
+    assert len(tr) >= 6
+    iv = [(ref.elapsed_time(t[2]), ref.elapsed_time(t[3])) for t in tr]
+    overlaps = sum(1 for i in range(len(iv)) for j in range(i + 1, len(iv))
+                   if iv[i][0] < iv[j][1] and iv[j][0] < iv[i][1])
+    assert overlaps >= 2, iv
+    srv.close()
+
+
+def test_small_request_finishes_before_a_large_one_submitted_earlier(gpu):
+    # a 1k-query request submitted behind a 10M-query request is answered
+    # first: the large one runs in slices, the small one on the fast slot
+    import torch
+    from pptk_b200 import serving
+    rng = np.random.default_rng(10)
+    cloud = torch.from_numpy(rng.random((2_000_000, 3), dtype=np.float32)).cuda()
+    srv = serving.Server(budget_bytes=16e9, slots=3)
+    tid = srv.build(cloud).result(timeout=120)
+    big_rows = torch.from_numpy(rng.integers(0, 2_000_000, 10_000_000).astype(np.int32)).cuda()
+    small_q = cloud[:1000] + 1e-3
+    torch.cuda.synchronize()
+    done = {}
+    big = srv.normals(tid, big_rows, k=16)
+    small = srv.knn(tid, small_q, k=16)
+    big.add_done_callback(lambda f: done.setdefault("big", time.perf_counter()))
+    small.add_done_callback(lambda f: done.setdefault("small", time.perf_counter()))
+    small.result(timeout=120)
+    big.result(timeout=120)
+    assert done["small"] < done["big"]
+    idx, _ = small.result()
+    direct, _ = gpu.kdtree.knn(srv.trees[tid], small_q, 16)
+    assert torch.equal(idx, direct)
     srv.close()
 
 

@@ -122,3 +122,130 @@ def test_knn_requests_of_one_k_class_share_a_launch():
     # k = 5 and 7 (capacity class 8) ran as one k = 7 launch; k = 20 on its own
     assert sorted(b[2] for b in launches) == [7, 20]
     srv.close()
+
+
+def wait_started(eng, kind, count=1, timeout=10.0):
+    """Waits until the engine has begun `count` batches of `kind`."""
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < timeout:
+        with eng.lock:
+            if sum(1 for b in eng.batches if b[0] == kind) >= count:
+                return
+        time.sleep(0.001)
+    raise TimeoutError(kind)
+
+
+class FailingEngine(FakeEngine):
+    """Raises in the batches whose first request has the marked size, as an
+    allocation refusal or a CUDA error of the native library would."""
+
+    def __init__(self, fail_m, exc, delay=0.0):
+        super().__init__(delay)
+        self.fail_m = fail_m
+        self.exc = exc
+
+    def knn_batch(self, trees, queries, k, dmax, stream, host=False):
+        if any(len(q) == self.fail_m for q in queries):
+            with self.lock:
+                self.batches.append(("knn-failed", len(trees), k))
+            raise self.exc
+        return super().knn_batch(trees, queries, k, dmax, stream, host)
+
+    def normals_batch(self, trees, indices, k, r, precision, stream, host=False):
+        if any(len(i) == self.fail_m for i in indices):
+            raise self.exc
+        return super().normals_batch(trees, indices, k, r, precision, stream, host)
+
+
+@pytest.mark.parametrize("exc", [MemoryError("device allocation refused"),
+                                 RuntimeError("CUDA error: an illegal memory access was encountered")])
+def test_a_failing_batch_fails_only_its_requests(exc):
+    eng = FailingEngine(fail_m=13, exc=exc, delay=0.02)
+    srv = serving.Server(budget_bytes=1e9, slots=1, engine=eng)
+    rng = np.random.default_rng(2)
+    pts = rng.random((100, 3))
+    tid = srv.build(pts).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((4, 3)), k=2)  # holds the only slot while the next ones queue
+    wait_started(eng, "knn")
+    bad = [srv.knn(tid, rng.random((13, 3)), k=3), srv.normals(tid, np.arange(13, dtype=np.int32), k=4)]
+    blocker.result(timeout=10)
+    for f in bad:
+        with pytest.raises(type(exc)):
+            f.result(timeout=10)
+    # the server keeps serving: later requests succeed
+    q = rng.random((7, 3))
+    idx, cnt = srv.knn(tid, q, k=3).result(timeout=10)
+    d = ((q[:, None, :] - pts[None]) ** 2).sum(-1)
+    assert np.array_equal(idx, np.argsort(d, axis=1, kind="stable")[:, :3])
+    assert srv.normals(tid, np.arange(9, dtype=np.int32), k=4).result(timeout=10).shape == (9, 3)
+    assert srv._committed == pytest.approx(100 * serving.TREE_BYTES_PER_POINT)
+    srv.close()
+
+
+def test_large_requests_are_answered_in_slices():
+    # a request above the batch cap runs as several batches; its answer is
+    # the same as in one piece
+    eng = FakeEngine(delay=0.0)
+    srv = serving.Server(budget_bytes=1e9, slots=2, engine=eng, max_batch_queries=64, min_batch_queries=1,
+                         small_batch=16)
+    rng = np.random.default_rng(3)
+    pts = rng.random((500, 3))
+    tid = srv.build(pts).result(timeout=10)
+    q = rng.random((300, 3))
+    idx, cnt = srv.knn(tid, q, k=4).result(timeout=10)
+    d = ((q[:, None, :] - pts[None]) ** 2).sum(-1)
+    assert np.array_equal(idx, np.argsort(d, axis=1, kind="stable")[:, :4]) and (cnt == 4).all()
+    assert len([b for b in eng.batches if b[0] == "knn"]) >= 300 // 64
+    ev = srv.normals(tid, None, k=4).result(timeout=10)
+    assert ev.shape == (500, 3)
+    srv.close()
+
+
+def test_small_request_overtakes_a_large_one():
+    # a small request submitted behind a large one is served by the fast
+    # slot while the large one's slices run on the other
+    eng = FakeEngine(delay=0.03)
+    srv = serving.Server(budget_bytes=1e9, slots=2, engine=eng, max_batch_queries=100, min_batch_queries=1,
+                         small_batch=50)
+    rng = np.random.default_rng(4)
+    tid = srv.build(rng.random((200, 3))).result(timeout=10)
+    big = srv.knn(tid, rng.random((1000, 3)), k=2)
+    time.sleep(0.01)
+    small = srv.knn(tid, rng.random((5, 3)), k=2)
+    small.result(timeout=10)
+    assert not big.done()
+    big.result(timeout=10)
+    st = srv.stats()
+    assert st["knn"]["requests"] == 2
+    srv.close()
+
+
+def test_cancelled_requests_never_run():
+    eng = FakeEngine(delay=0.05)
+    srv = serving.Server(budget_bytes=1e9, slots=1, engine=eng)
+    rng = np.random.default_rng(5)
+    tid = srv.build(rng.random((100, 3))).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((3, 3)), k=2)
+    wait_started(eng, "knn")
+    doomed = srv.knn(tid, rng.random((11, 3)), k=2)
+    kept = srv.knn(tid, rng.random((6, 3)), k=2)
+    assert doomed.cancel()
+    blocker.result(timeout=10)
+    idx, _ = kept.result(timeout=10)
+    assert idx.shape == (6, 2) and doomed.cancelled()
+    with eng.lock:
+        sizes = [b for b in eng.batches if b[0] == "knn"]
+    assert len(sizes) == 2  # the blocker and the kept request; the cancelled one never ran
+    srv.close()
+
+
+def test_batch_cap_follows_the_measured_rate():
+    eng = FakeEngine(delay=0.0)
+    srv = serving.Server(budget_bytes=1e9, slots=1, engine=eng, max_batch_queries=10_000_000,
+                         min_batch_queries=1000, batch_ms=10.0)
+    assert srv.batch_cap() == 10_000_000  # no rate measured yet: the upper bound
+    srv._rate = 2e8
+    assert srv.batch_cap() == 2_000_000
+    srv._rate = 1e4
+    assert srv.batch_cap() == 1000  # never below the lower bound
+    srv.close()
