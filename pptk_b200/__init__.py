@@ -7,8 +7,8 @@ hand-written sm_100a CUDA kernels behind the C ABI of ``include/pptkg.h``.
 """
 from . import kdtree
 from .estimate_normals import estimate_normals
-from .pca import eigh3, nbhd_pca
+from .pca import eigh3, eigh_list, nbhd_pca
 from .points import Points, points
 
-__all__ = ["kdtree", "estimate_normals", "eigh3", "nbhd_pca", "Points", "points"]
+__all__ = ["kdtree", "estimate_normals", "eigh3", "eigh_list", "nbhd_pca", "Points", "points"]
 __version__ = "0.1.0"

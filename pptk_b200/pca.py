@@ -39,6 +39,39 @@ def eigh3(A, layout="columns"):
     return w, V
 
 
+def eigh_list(X):
+    """The calling form of vfuncs ``_eigh`` (pptk/vfuncs/vfuncs.cpp:1241-1293)
+    over the batched GPU solve: X is a non-empty list of square float32
+    arrays; returns a list of (w, V) pairs, float32, w ascending and
+    ``V[:, j]`` the j-th eigenvector (the reference copies Eigen's row-major
+    eigenvector matrix element by element, :1285-1287).  As Eigen's
+    SelfAdjointEigenSolver does, only the lower triangle of each matrix is
+    read.  The GPU path solves 3 x 3 blocks (the neighbourhood covariances
+    of the expression layer, pptk/points/expr.py:27-72); other sizes raise
+    NotImplementedError."""
+    if not isinstance(X, list):
+        raise TypeError("eigh_list: a list of arrays is required")
+    if not X:
+        raise ValueError("eigh_list: the list must not be empty")
+    blocks = np.empty((len(X), 3, 3), np.float32)
+    for i, a in enumerate(X):
+        if not isinstance(a, np.ndarray):
+            raise TypeError(f"eigh_list: item {i} is not a numpy array")
+        if a.dtype != np.float32:
+            raise TypeError(f"eigh_list: item {i} must be float32")
+        if a.ndim not in (1, 2):
+            raise ValueError(f"eigh_list: item {i} must have 1 or 2 dimensions")
+        rows, cols = (1, a.shape[0]) if a.ndim == 1 else a.shape
+        if rows != cols:
+            raise ValueError(f"eigh_list: item {i} is not square ({rows} x {cols})")
+        if rows != 3:
+            raise NotImplementedError(f"eigh_list: item {i} is {rows} x {rows}; the GPU path solves 3 x 3 blocks")
+        low = np.tril(a)
+        blocks[i] = low + np.tril(a, -1).T
+    w, V = eigh3(blocks, layout="columns")
+    return [(w[i].copy(), V[i].copy()) for i in range(len(X))]
+
+
 def _csr(nbhds):
     """(offsets int64 m+1, indices int32) from a list of index arrays (the
     _query / Points.nbhds form), a (offsets, indices) pair, or a dense

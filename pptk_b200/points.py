@@ -1,14 +1,22 @@
 """Points with a cached device k-d tree: the hot-path callers of pptk's
-``_query`` (pptk/points/points.py:140-166, expr.py:397-424).
+``_query`` (pptk/points/points.py:87-181 for the class, expr.py:397-424 for
+the lazy neighbourhood operator).
 
-``Points`` is an ndarray subclass, read-only except through its own
-in-place operators and item assignment, which record the time of every
-change of the underlying buffer.  Its k-d tree is built on the GPU the first
-time it is needed and rebuilt whenever the buffer changed after the last
-build (``_update_kd_tree``).  ``nbhds`` answers exactly like
-``kdtree._query`` on that tree; ``NBHDS`` returns a lazy neighbourhood
-expression that evaluates in chunks; ``nbhds_dense`` gives the dense
-(indices, counts) form without building per-query lists.
+Design.  Every memory buffer that Points arrays live in has one
+``_Generation`` record, shared by all Points views of that buffer.  Points
+are read-only to plain numpy writes; their own writers (item assignment and
+the in-place operators) unlock the buffer for the duration of the write and
+then advance the record's generation number.  A Points object keeps the
+device tree it built last, tagged with the generation it was built at;
+``_update_kd_tree`` rebuilds exactly when the generation moved on.  The
+observable behaviour is the reference's (a tree follows every write made
+through any view of the buffer, and nothing is rebuilt otherwise), without
+wall-clock timestamps: two writes in the same clock tick cannot be missed.
+
+``nbhds`` answers exactly like ``kdtree._query`` on the current tree;
+``NBHDS`` returns a lazy neighbourhood expression that evaluates in chunks;
+``nbhds_dense`` gives the dense (indices, counts) form without building
+per-query lists.
 """
 import time
 
@@ -16,52 +24,87 @@ import numpy as np
 
 from . import kdtree
 
-__all__ = ["Points", "points", "nbhds_op"]
+__all__ = ["Points", "points", "nbhds_op", "zeros", "ones", "empty", "zeros_like", "ones_like", "empty_like",
+           "rand", "load"]
+
+
+class _Generation:
+    """Write counter of one buffer: [lo, hi) are its byte addresses."""
+    __slots__ = ("lo", "hi", "value")
+
+    def __init__(self, lo, nbytes):
+        self.lo, self.hi, self.value = lo, lo + nbytes, 0
+
+    def covers(self, addr):
+        return self.lo <= addr < self.hi
+
+
+def _address(a):
+    return a.__array_interface__["data"][0]
 
 
 class Points(np.ndarray):
-    _last_modified = {}
+    """An (n, dim) point array whose k-d tree lives on the GPU and follows
+    the array's contents.  Plain numpy writes are refused (the array is not
+    writeable); item assignment and in-place arithmetic on the Points object
+    itself are allowed and mark the buffer as changed."""
 
-    def __new__(cls, *args, **kwargs):
-        return super().__new__(cls, *args, **kwargs)
-
-    def __array_finalize__(self, obj):
-        self._last_updated = None
+    def __array_finalize__(self, parent):
         self._tree = None
-        if obj is not None and not isinstance(obj, Points):
-            raise TypeError("Detected attempt at creating Points-type view on non-Points object.")
-        base = self.__array_interface__["data"][0]
-        if obj is None or base < obj._memloc or base >= obj._memloc + obj._memsize:
-            # a new buffer (construction or copy)
-            self._memsize = self.size * self.dtype.itemsize
-            self._memloc = base
+        self._tree_generation = -1
+        if parent is not None and not isinstance(parent, Points):
+            # ndarray.view(Points): a plain array cannot report its writes
+            raise TypeError("a Points view can only be taken of a Points array; use points(a) to make a copy")
+        addr = _address(self)
+        gen = getattr(parent, "_gen", None)
+        if gen is not None and gen.covers(addr):
+            self._gen = gen  # a slice or view: the same buffer, the same counter
         else:
-            # a view into obj's buffer: share its modification record
-            self._memsize = obj._memsize
-            self._memloc = obj._memloc
+            self._gen = _Generation(addr, self.nbytes)  # a new buffer (construction, copy, ufunc output)
 
     def __init__(self, *args, **kwargs):
         self.flags.writeable = False
 
     def copy(self, order="C"):
-        x = super().copy(order)
-        x.flags.writeable = False
-        return x
+        out = super().copy(order)
+        out.flags.writeable = False
+        return out
 
-    def _record_modify_time(self):
-        Points._last_modified[self._memloc] = time.time()
+    # -------------------------------------------------------------- writes --
+    def _owner(self):
+        b = self.base
+        return b if isinstance(b, np.ndarray) else None
 
+    def _write(self, fn, *args):
+        """Runs a write with the buffer unlocked, then advances its
+        generation (also when the write raised part way)."""
+        owner = self._owner()
+        if owner is not None:
+            owner.flags.writeable = True
+        self.flags.writeable = True
+        try:
+            return fn(*args)
+        finally:
+            self.flags.writeable = False
+            if owner is not None:
+                owner.flags.writeable = False
+            self._gen.value += 1
+
+    def __setitem__(self, key, value):
+        self._write(super().__setitem__, key, value)
+
+    # -------------------------------------------------------------- trees --
     def _update_kd_tree(self):
-        """(Re)builds the device tree if the buffer changed since the last
-        build; returns the build time in seconds, or None if none was needed."""
-        if Points._last_modified.get(self._memloc) is None:
-            Points._last_modified[self._memloc] = time.time()
-        if self._last_updated is None or self._last_updated <= Points._last_modified[self._memloc]:
-            t0 = time.time()
-            self._tree = kdtree._build(np.ascontiguousarray(self.view(np.ndarray)))
-            self._last_updated = time.time()
-            return self._last_updated - t0
-        return None
+        """Builds the device tree if none exists or the buffer was written
+        since the last build; returns the build time in seconds, or None
+        when the cached tree is current."""
+        if self._tree is not None and self._tree_generation == self._gen.value:
+            return None
+        gen = self._gen.value
+        t0 = time.perf_counter()
+        self._tree = kdtree._build(np.ascontiguousarray(self.view(np.ndarray)))
+        self._tree_generation = gen
+        return time.perf_counter() - t0
 
     def nbhds(self, queries=None, k=1, r=None, verbose=False):
         """Neighbourhoods as kdtree._query returns them (a list of index
@@ -78,54 +121,79 @@ class Points(np.ndarray):
     def NBHDS(self, queries=None, k=1, r=None, verbose=False):
         return nbhds_op(self, queries, k, r)
 
-    def _guard(self, f):
-        def guarded(*args, **kwargs):
-            if self.base is not None and isinstance(self.base, np.ndarray):
-                self.base.flags.writeable = True
-            self.flags.writeable = True
-            try:
-                return f(*args, **kwargs)
-            finally:
-                self.flags.writeable = False
-                if self.base is not None and isinstance(self.base, np.ndarray):
-                    self.base.flags.writeable = False
-                self._record_modify_time()
-        return guarded
-
-    def __setitem__(self, key, value):
-        return self._guard(super().__setitem__)(key, value)
-
-    def __delitem__(self, key):
-        return self._guard(super().__delitem__)(key)
-
 
 def _inplace(name):
+    base = getattr(np.ndarray, name)
+
     def op(self, other):
-        return self._guard(getattr(np.ndarray, name).__get__(self))(other)
+        return self._write(base, self, other)
+
     op.__name__ = name
+    op.__doc__ = f"In-place {name[3:-2]} that marks the buffer as changed."
     return op
 
 
+# += -= *= /= //= %= **= <<= >>= &= ^= |= and @= all go through _write
 for _name in ("__iadd__", "__isub__", "__imul__", "__itruediv__", "__ifloordiv__", "__imod__", "__ipow__",
-              "__ilshift__", "__irshift__", "__iand__", "__ixor__", "__ior__"):
+              "__ilshift__", "__irshift__", "__iand__", "__ixor__", "__ior__", "__imatmul__"):
     setattr(Points, _name, _inplace(_name))
 
 
+# ------------------------------------------------------------ construction --
+def empty(shape, dtype=float):
+    return Points(shape=shape, dtype=dtype)
+
+
+def zeros(shape, dtype=float):
+    out = empty(shape, dtype)
+    out[...] = 0
+    return out
+
+
+def ones(shape, dtype=float):
+    out = empty(shape, dtype)
+    out[...] = 1
+    return out
+
+
+def empty_like(a, dtype=None):
+    return zeros(np.shape(a), a.dtype if dtype is None else dtype)
+
+
+def zeros_like(a, dtype=None):
+    return zeros(np.shape(a), a.dtype if dtype is None else dtype)
+
+
+def ones_like(a, dtype=None):
+    return ones(np.shape(a), a.dtype if dtype is None else dtype)
+
+
+def rand(*dims):
+    out = empty(dims, float)
+    out[...] = np.random.rand(*dims)
+    return out
+
+
 def points(object, dtype=None, copy=True):
-    """A Points copy of `object` (or a Points view of an ndarray when
-    copy=False and no conversion is needed)."""
-    if not copy and isinstance(object, np.ndarray) and (dtype is None or dtype == object.dtype):
+    """A Points copy of `object`.  With copy=False a Points array is
+    returned as a view of itself when no conversion is needed."""
+    if not copy and isinstance(object, Points) and (dtype is None or dtype == object.dtype):
         return object.view(Points)
-    temp = np.asarray(object, dtype=dtype)
-    ret = Points(shape=temp.shape, dtype=temp.dtype)
-    ret[:] = temp
-    return ret
+    src = np.asarray(object, dtype=dtype)
+    out = empty(src.shape, src.dtype)
+    out[...] = src
+    return out
+
+
+def load(file, **kwargs):
+    """numpy.load into a Points array."""
+    return points(np.load(file, **kwargs))
 
 
 class nbhds_op:
     """Lazy neighbourhoods of a Points object (expr.py:397-424): len() is the
     number of queries; evaluate() (or _evaluate_chunk) runs the query on the
-    cached device tree."""
+    object's current device tree."""
 
     def __init__(self, data, queries, k, r):
         self.data = data
@@ -138,10 +206,7 @@ class nbhds_op:
 
     def _evaluate_chunk(self, index, size, use_cache=False):
         self.data._update_kd_tree()
-        if self.queries is None:
-            q = np.arange(index, index + size)
-        else:
-            q = self.queries[index:index + size]
+        q = np.arange(index, index + size) if self.queries is None else self.queries[index:index + size]
         return kdtree._query(self.data._tree, q, self.k, self.r)
 
     def evaluate(self, chunk=1_000_000):

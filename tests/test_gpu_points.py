@@ -64,3 +64,32 @@ def test_nbhd_pca_matches_float64(gpu):
     assert np.array_equal(C1, C2)
     with pytest.raises(RuntimeError):
         pca.nbhd_covariance(X, [np.array([0, 30_000])])
+
+
+def test_eigh_list_matches_lapack(gpu):
+    # vfuncs._eigh's calling form: a list of float32 3 x 3 arrays in, a list
+    # of (w, V) pairs out with V[:, j] the j-th eigenvector; only the lower
+    # triangle is read
+    from pptk_b200 import pca
+    rng = np.random.default_rng(2)
+    X = []
+    for i in range(500):
+        Y = rng.normal(size=(3, 3))
+        A = (Y @ Y.T).astype(np.float32)
+        if i % 5 == 0:
+            A = np.asfortranarray(A)  # any memory layout
+        if i % 7 == 0:
+            A[0, 2] += np.float32(5.0)  # the upper triangle is ignored
+        X.append(A)
+    out = pca.eigh_list(X)
+    assert isinstance(out, list) and len(out) == len(X)
+    for A, (w, V) in zip(X, out):
+        assert w.dtype == np.float32 and V.dtype == np.float32 and w.shape == (3,) and V.shape == (3, 3)
+        S = np.tril(A).astype(np.float64)
+        S = S + np.tril(S, -1).T
+        wl, Vl = np.linalg.eigh(S)
+        assert np.allclose(w, wl, rtol=1e-5, atol=1e-5 * np.abs(wl).max())
+        gap = np.diff(wl) / max(np.abs(wl).max(), 1e-30)
+        for j in range(3):
+            if (j == 0 or gap[j - 1] > 1e-3) and (j == 2 or gap[j] > 1e-3):
+                assert abs(float(V[:, j].astype(np.float64) @ Vl[:, j])) > 1 - 1e-5

@@ -139,16 +139,55 @@ def test_synthetic_workloads_are_seeded():
 
 
 def test_points_track_writes_through_views():
+    import importlib
+    PM = importlib.import_module("pptk_b200.points")
     from pptk_b200.points import Points, points
     P = points(np.zeros((10, 3), np.float32))
     assert not P.flags.writeable
     with pytest.raises(ValueError):
         np.ndarray.__setitem__(P, 0, 1.0)  # plain writes are refused
-    t0 = Points._last_modified[P._memloc]
+    g0 = P._gen.value
     v = P[2:5]
-    assert v._memloc == P._memloc  # a view shares the buffer's record
+    assert v._gen is P._gen  # a view shares the buffer's write counter
     v += 1
-    assert Points._last_modified[P._memloc] >= t0 and P[2, 0] == 1.0
+    assert P._gen.value > g0 and P[2, 0] == 1.0 and not v.flags.writeable
+    v[0, 1] = 7.0
+    assert P[2, 1] == 7.0 and P._gen.value > g0 + 1
     c = P.copy()
-    assert c._memloc != P._memloc and not c.flags.writeable
+    assert c._gen is not P._gen and not c.flags.writeable
+    with pytest.raises(TypeError):
+        np.zeros((4, 3)).view(Points)  # a plain array cannot report its writes
     assert len(P.NBHDS(queries=[1, 2, 3], k=2)) == 3
+    # every in-place operator marks the buffer
+    for op in ("__iadd__", "__isub__", "__imul__", "__itruediv__", "__ipow__"):
+        g = P._gen.value
+        getattr(P, op)(np.float32(1.0))
+        assert P._gen.value == g + 1, op
+    Q = points(np.arange(12, dtype=np.int32).reshape(4, 3))
+    for op in ("__ifloordiv__", "__imod__", "__ilshift__", "__irshift__", "__iand__", "__ixor__", "__ior__"):
+        g = Q._gen.value
+        getattr(Q, op)(np.int32(1))
+        assert Q._gen.value == g + 1, op
+    # constructors
+    assert (PM.zeros((2, 3)) == 0).all() and (PM.ones((2, 3)) == 1).all() and PM.empty((2, 3)).shape == (2, 3)
+    assert (PM.ones_like(P) == 1).all() and PM.zeros_like(P).dtype == P.dtype and PM.rand(3, 3).shape == (3, 3)
+    assert isinstance(PM.points(P, copy=False), Points) and PM.points(P, copy=False)._gen is P._gen
+
+
+def test_eigh_list_argument_errors():
+    # checked before any device work (vfuncs.cpp:1241-1270 contract)
+    from pptk_b200 import pca
+    with pytest.raises(TypeError):
+        pca.eigh_list(np.eye(3, dtype=np.float32))
+    with pytest.raises(ValueError):
+        pca.eigh_list([])
+    with pytest.raises(TypeError):
+        pca.eigh_list([np.eye(3)])  # float64
+    with pytest.raises(TypeError):
+        pca.eigh_list([[1.0, 0.0]])
+    with pytest.raises(ValueError):
+        pca.eigh_list([np.zeros((2, 3), np.float32)])
+    with pytest.raises(ValueError):
+        pca.eigh_list([np.zeros((1, 3, 3), np.float32)])
+    with pytest.raises(NotImplementedError):
+        pca.eigh_list([np.eye(4, dtype=np.float32)])
