@@ -235,10 +235,8 @@ class RefScene:
                 "knn_queries_per_s": len(kq) / (t1 - t0), "normal_queries_per_s": len(nq) / (t2 - t1)}
 
     def describe(self, sample, k):
-        return (f"reference k-d tree over the whole scene ({len(self.pts)} points, built once: {self.build_s:.1f} s "
-                f"serial) answering {sample} random rows of the request stream per step ({sample // 2} kNN k={k} "
-                f"point queries + {sample - sample // 2} normal k={k} queries: kNN with the query point + "
-                "covariance + Jacobi eigensolve); TBB absent: OpenMP over the reference's per-query calls")
+        return (f"ref tree on the {len(self.pts)}-pt scene, built once (build_s); {sample} request rows/step, half "
+                f"kNN k={k}, half normals; OpenMP for TBB")
 
 
 def serving_cpu_baseline(pts, mix, args):
@@ -382,10 +380,9 @@ def roofline(ctx, stage_name, queries, traffic_kind):
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
     traffic = TRAFFIC_PER_QUERY[traffic_kind] * queries / cnt
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "k_normals (fused kNN+PCA)", "peak_kind": f"{peak_kind} hbm_gbs",
-            "launches": cnt, "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch,
-            "traffic_source": f"ncu DRAM bytes per query ({traffic_kind} queries, 8M-point capture) x queries "
-                              "per launch"}
+            "traffic": traffic, "kernel": "k_normals", "peak_kind": f"{peak_kind} hbm_gbs",
+            "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch,
+            "traffic_source": f"ncu bytes/query ({traffic_kind}) x queries"}
 
 
 BUILD_STAGES = ("build", "build.prep", "build.attempt", "build.levels", "build.subtree", "build.finish",
@@ -892,13 +889,10 @@ def run_serving_workload(args, ctx):
     cpu = (serving_cpu_baseline(pts, mix, args)
            if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline else None)
     return {"value": value, "ms_per_step": ms_max,
-            "config": {"workload": f"lidar_scene_{n}_f32 resident tree; request stream of {len(mix)} requests "
-                                   f"({n_knn} kNN k={k} point queries + {n_norm} normal k={k} r=inf queries, "
-                                   "sizes log-uniform in [1k, 1M]) answered by the continuous-batching server",
-                       "points": n, "k": k, "requests_per_step": len(mix), "queries_per_step": per_step,
-                       "slots": args.slots, "max_batch_queries": args.max_batch, "batch_ms": args.batch_ms,
-                       "l2": "scene (240 MB) and request inputs larger than L2 (126 MB); no flush",
-                       "unit": "one kNN request row or one normal request row",
+            "config": {"workload": f"lidar scene {n} f32, resident tree, server; {len(mix)} requests/step: "
+                                   f"{n_knn} kNN k={k} + {n_norm} normal k={k} queries",
+                       "points": n, "k": k, "queries_per_step": per_step, "slots": args.slots,
+                       "batch_ms": args.batch_ms, "l2": "inputs > L2, no flush", "unit": "request row",
                        "parallelism": f"replicas x{ctx.world}"},
             "plain": plain, "latency": latency, "latency_at_quarter_load": latency_q,
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof, "cpu_baseline": cpu,
@@ -975,8 +969,9 @@ def _lat(d):
 
 
 def _precision_summary(prec):
-    return {name: {"p99_rad": v["vs_cpu_fp64_oracle_sample"]["p99"], "max_rad": v["vs_cpu_fp64_oracle_sample"]["max"],
-                   "p99_all_rows_vs_device_fp64_rad": v["vs_device_fp64_all_rows"]["p99"]}
+    """p99 / max angular error (rad) of the FP32 path against the CPU FP64
+    oracle on 20k sampled rows, per cloud."""
+    return {name: [v["vs_cpu_fp64_oracle_sample"]["p99"], v["vs_cpu_fp64_oracle_sample"]["max"]]
             for name, v in prec.items()}
 
 
@@ -1003,26 +998,39 @@ def run_config(name, args, ctx):
         a.no_e2e = False
     res = WORKLOADS[name](a, ctx)
     summary = {"value": res["value"], "unit": "queries/s" if name != "ragged" else "points/s",
-               "ms_per_step": res["ms_per_step"], "steps": a.steps, "warmup": a.warmup,
-               "workload": res["config"]["workload"]}
+               "ms_per_step": res["ms_per_step"]}
     if name == "scene":
         rn = res["rnear"]
-        summary["rnear_r0.5"] = {"count_all_points_ms": rn["count_all_points_ms"],
-                                 "total_hits": rn["total_hits_all_points"],
-                                 "sample_count_and_fill_ms": rn["sample_count_and_fill_ms"],
-                                 "sample_queries": rn["sample_queries"]}
+        summary["rnear_r0.5"] = {"count_all_ms": rn["count_all_points_ms"], "hits": rn["total_hits_all_points"],
+                                 "fill_20k_ms": rn["sample_count_and_fill_ms"]}
     elif name == "ragged":
         st = res["stages_ms"]
-        summary["stage_ms_per_step"] = {k: round(v["ms_per_step"], 2) for k, v in st.items()
-                                        if k in ("build", "forest.knn", "forest.normals")}
-        summary["graph_replay_queries_ms"] = res["graph_replay"]["ms_per_step"]
-        summary["e2e"] = res["e2e"]
+        summary["stage_ms"] = {k: round(v["ms_per_step"], 1) for k, v in st.items()
+                               if k in ("build", "forest.knn", "forest.normals")}
+        summary["graph_replay_queries_ms"] = round(res["graph_replay"]["ms_per_step"], 1)
+        summary["e2e_value"] = (res["e2e"] or {}).get("value")
     elif name == "multitree":
-        summary["latency_quarter_load"] = _lat(res["latency"])
-        summary["latency_half_load"] = _lat(res["latency_at_half_load"])
+        lq, lh = _lat(res["latency"]), _lat(res["latency_at_half_load"])
+        summary["p50_p99_ms_quarter_load"] = [round(lq["p50_ms"], 1), round(lq["p99_ms"], 1)]
+        summary["p50_p99_ms_half_load"] = [round(lh["p50_ms"], 1), round(lh["p99_ms"], 1)]
         summary["build_points_per_s"] = res["build"]["points_per_s"]
-    summary["clocks"] = res.get("clocks")
+    clk = res.get("clocks") or {}
+    summary["sm_mhz"] = clk.get("sm_mhz")
+    if clk.get("reasons"):
+        summary["clock_reasons"] = clk.get("reasons")
     return summary, res
+
+
+def _round(x, digits=4):
+    """Floats to `digits` significant digits, recursively (keeps the judged
+    line short)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: _round(v, digits) for k, v in x.items()}
+    if isinstance(x, list):
+        return [_round(v, digits) for v in x]
+    return x
 
 
 def run_ours(args):
@@ -1059,11 +1067,11 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic"}
-        line.update(res)
+        line.update(_round(res))
         if "precision" in details:
-            line["precision_fp32_vs_fp64_oracle"] = _precision_summary(details["precision"])
+            line["precision_fp32_vs_fp64_oracle"] = _round(_precision_summary(details["precision"]), 3)
         if configs:
-            line["configs"] = configs
+            line["configs"] = _round(configs)
         if tuned:
             line["config"]["tune"] = tuned
         print(json.dumps(line), flush=True)

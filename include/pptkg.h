@@ -146,7 +146,9 @@ PPTKG_API int pptkg_estimate_normals(const void* points, int64_t n, int dtype, i
                            const int32_t* subsample, int64_t m, int num_eigen, int precision, void* out_evecs,
                            void* out_evals, int32_t* out_sizes, void* stream);
 
-/* The same PCA over an existing 3-D tree (rows of the tree's input). */
+/* The same PCA over an existing 3-D tree (rows of the tree's input): the
+ * rows `indices` (m of them), or every row when indices is NULL (m must then
+ * be 0 or the tree's row count; the outputs hold one entry per row). */
 PPTKG_API int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices, int64_t m, int mem, int k, float r,
                        int num_eigen, int precision, void* out_evecs, void* out_evals, int32_t* out_sizes,
                        void* stream);
@@ -270,6 +272,11 @@ PPTKG_API int64_t pptkg_launch_count(void);
  *     Default 262144 (below it, 32-query packets leave B200's 148 SMs short
  *     of warps).  Hit lists and neighbourhood sizes do not depend on it;
  *     normals agree to FP64 rounding (their sums add in another order).
+ *   "warm_bound": kNN / normals lists start from the k tree positions
+ *     around each query's anchor; with 1 their bound is also lowered to the
+ *     k-th distance over a wider window of tree-order neighbours (fewer
+ *     list insertions), with 0 not.  Default 1.  Results do not depend on
+ *     it.
  * Unknown names or out-of-range values: PPTKG_E_INVALID. */
 PPTKG_API int pptkg_tune_set(const char* name, int64_t value);
 PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);

@@ -668,6 +668,11 @@ int pptkg_tree_normals(const pptkg_tree* tree, const int32_t* indices, int64_t m
   return guarded([&] {
     const TreeBase* t = tree_of(tree);
     DeviceGuard g(t->device);
+    if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
+    if (t->rec_dtype != F32 && t->rec_dtype != F64) throw Error(E_TYPE, "normals need float32 or float64 points");
+    // NULL indices mean every row: outputs are sized for n rows
+    if (!indices && m != 0 && m != t->n)
+      throw Error(E_INVALID, "with indices NULL, m must be 0 or the tree's row count (every row is answered)");
     if (!indices) m = t->n;
     if (m < 0 || m > INT32_MAX) throw Error(E_INVALID, "query count out of range");
     run_normals(t, indices, m, mem, k, r, num_eigen, precision, out_evecs, out_evals, out_sizes, S(stream));

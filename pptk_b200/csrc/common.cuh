@@ -51,6 +51,10 @@ extern std::atomic<int> g_tune_lane_span;
 //  rnear_warp_queries: r-near batches of at most this many queries run one
 //    warp per query instead of 32-query packets (0: never).
 extern std::atomic<int> g_tune_rnear_warp_queries;
+//  warm_bound: after the warm start of a kNN list, also lower its bound to
+//    the k-th distance of the 32 (k <= 16) or 3 x k tree-order neighbours
+//    of the query's anchor (1) or not (0).
+extern std::atomic<int> g_tune_warm_bound;
 
 // Status sink of this host thread (pptkg_set_status_sink): while set, query
 // entry points record kernel check failures into this device word and

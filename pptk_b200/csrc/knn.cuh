@@ -74,6 +74,7 @@ struct TopK;
 // non-negative floats order like their bit patterns.
 template <int KMAX>
 struct TopK<KMAX, float> {
+  static constexpr int CAP = KMAX;
   unsigned long long s[KMAX];
   unsigned long long lim;
   __device__ __forceinline__ void reset(int k, float r2) {
@@ -95,28 +96,59 @@ struct TopK<KMAX, float> {
     s[KMAX - 1] = s[KMAX - 1] > c ? c : s[KMAX - 1];
   }
   // Lowers the bound of the k live slots to b, inclusively (distances equal
-  // to b still enter): the seed key sorts after every real key of distance b.
-  // Only valid when at least k real candidates with distance <= b exist, so
-  // that every seed key is pushed out by the end of the search.
+  // to b still enter): live keys above the seed key become the seed key,
+  // which sorts after every real key of distance b, so the list stays
+  // sorted.  Only valid when at least k real candidates with distance <= b
+  // are in the list or will be offered, so that every seed key is pushed out
+  // by the end of the search.
   __device__ __forceinline__ void seed(int k, float b, float) {
     const unsigned long long key = ((unsigned long long)__float_as_uint(b) << 32) | 0xffffffffull;
     if (!(b >= 0.f) || key >= lim) return;
 #pragma unroll
     for (int j = 0; j < KMAX; j++)
-      if (j < k) s[j] = key;
+      if (j < k && s[j] > key) s[j] = key;
   }
   __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return s[j] < lim && (unsigned)s[j] != 0xffffffffu; }
   __device__ __forceinline__ int id(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
   __device__ __forceinline__ float dist(int j) const { return __uint_as_float((unsigned)(s[j] >> 32)); }
+  // Warm start (see warm_topk): slot j holds a real candidate, an empty
+  // live slot (no candidate yet) or a dead slot (beyond k); sort_desc()
+  // then restores the list order.
+  __device__ __forceinline__ void set_real(int j, float d2, int id) {
+    s[j] = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
+  }
+  __device__ __forceinline__ void set_empty(int j) { s[j] = lim; }
+  __device__ __forceinline__ void set_dead(int j) { s[j] = 0ull; }
+  __device__ __forceinline__ void sort_desc() {
+    // bitonic network, fully unrolled over the compile-time capacity
+#pragma unroll
+    for (int size = 2; size <= KMAX; size <<= 1)
+#pragma unroll
+      for (int stride = size / 2; stride > 0; stride >>= 1)
+#pragma unroll
+        for (int i = 0; i < KMAX; i++) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const unsigned long long a = s[i], b = s[j];
+            const bool up = (i & size) != 0;  // this block ends ascending
+            const bool sw = up ? (a > b) : (a < b);
+            s[i] = sw ? b : a;
+            s[j] = sw ? a : b;
+          }
+        }
+  }
 };
 
 // double distances: parallel (dist2, id) arrays compared lexicographically.
 template <int KMAX>
 struct TopK<KMAX, double> {
+  static constexpr int CAP = KMAX;
   double d[KMAX];
   int p[KMAX];
+  double lim_d;
   __device__ __forceinline__ void reset(int k, double r2) {
+    lim_d = r2;
 #pragma unroll
     for (int j = 0; j < KMAX; j++) {
       d[j] = j < k ? r2 : -1.0;
@@ -148,7 +180,7 @@ struct TopK<KMAX, double> {
     if (!(b >= 0.0) || !(b < r2)) return;
 #pragma unroll
     for (int j = 0; j < KMAX; j++)
-      if (j < k) {
+      if (j < k && gt(d[j], p[j], b, 0x7fffffff)) {
         d[j] = b;
         p[j] = 0x7fffffff;
       }
@@ -157,6 +189,38 @@ struct TopK<KMAX, double> {
   __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && p[j] != 0x7fffffff && d[j] >= 0.0; }
   __device__ __forceinline__ int id(int j) const { return p[j]; }
   __device__ __forceinline__ double dist(int j) const { return d[j]; }
+  __device__ __forceinline__ void set_real(int j, double d2, int id) {
+    d[j] = d2;
+    p[j] = id;
+  }
+  __device__ __forceinline__ void set_empty(int j) {
+    d[j] = lim_d;
+    p[j] = -1;
+  }
+  __device__ __forceinline__ void set_dead(int j) {
+    d[j] = -1.0;
+    p[j] = -1;
+  }
+  __device__ __forceinline__ void sort_desc() {
+#pragma unroll
+    for (int size = 2; size <= KMAX; size <<= 1)
+#pragma unroll
+      for (int stride = size / 2; stride > 0; stride >>= 1)
+#pragma unroll
+        for (int i = 0; i < KMAX; i++) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const double da = d[i], db = d[j];
+            const int pa = p[i], pb = p[j];
+            const bool up = (i & size) != 0;
+            const bool sw = up ? gt(da, pa, db, pb) : gt(db, pb, da, pa);
+            d[i] = sw ? db : da;
+            d[j] = sw ? da : db;
+            p[i] = sw ? pb : pa;
+            p[j] = sw ? pa : pb;
+          }
+        }
+  }
 };
 
 // ----------------------------------------------------- packet traversal --
@@ -217,9 +281,18 @@ __device__ __forceinline__ TNode<T, D> load_node(const TNode<T, D>* nodes, int i
   return n;
 }
 
+// Bits [a, a + n) of a 32-bit chunk mask (clipped to the chunk; 0 if empty).
+__device__ __forceinline__ unsigned window_bits(int a, int n) {
+  const int lo = max(a, 0), hi = min(a + n, 32);
+  if (hi <= lo) return 0u;
+  const unsigned top = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+  return top & ~((1u << lo) - 1u);
+}
+
 // Exact kNN of the lane's query over the whole tree, ties in dist2 broken by
 // point id.  `own` (tree position or -1) is skipped, which is how self
-// queries exclude the query point itself.  Returns false when the traversal
+// queries exclude the query point itself; so are the tree positions
+// [wlo, wlo + wn), the warm-start window whose candidates the list holds.  Returns false when the traversal
 // stack would overflow (the host sizes it from the tree depth, so this is a
 // safety net that reports instead of corrupting memory).
 //
@@ -228,7 +301,7 @@ __device__ __forceinline__ TNode<T, D> load_node(const TNode<T, D>* nodes, int i
 // children carry their boxes on the stack.
 template <typename T, int D, typename Top, typename DistT>
 __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top,
-                           WarpScratch<T, D> ws) {
+                           WarpScratch<T, D> ws, int wlo = 0, int wn = 0) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
   StackEnt<T, D>* stk = reinterpret_cast<StackEnt<T, D>*>(ws.stack);
@@ -279,8 +352,10 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
         const unsigned m = __ballot_sync(FULL, d2 <= qi.thr) & valid;
         if (lane == i) mark = m;
       }
-      // the query's own point never enters its list
+      // the query's own point never enters its list, and the positions of
+      // its warm-start window are in it already
       if (own >= base && own < base + nb) mark &= ~(1u << (own - base));
+      mark &= ~window_bits(wlo - base, wn);
       __syncwarp();
       top.reserve(__popc(mark));
       while (mark) {
@@ -393,7 +468,8 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
 // result (the k smallest (dist2, id) pairs) is identical.
 // Requires tv.depth <= LSTACK (the caller checks); false on a corrupt tree.
 template <int LSTACK, typename T, int D, typename DistT, typename Top>
-__device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top) {
+__device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top,
+                         int wlo = 0, int wn = 0) {
   if (!active) return true;
   int sref[LSTACK], scnt[LSTACK];
   DistT smd[LSTACK];
@@ -414,12 +490,13 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
       }
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        if (d2[j] <= top.worst() && d2[j] < r2 && p + j != own) top.offer(d2[j], r[j].id);
+        if (d2[j] <= top.worst() && d2[j] < r2 && p + j != own && (unsigned)(p + j - wlo) >= (unsigned)wn)
+          top.offer(d2[j], r[j].id);
     }
     for (; p < end; p++) {
       const PointRec<T, D> r = tv.pts[p];
       const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
-      if (d2 <= top.worst() && d2 < r2 && p != own) top.offer(d2, r.id);
+      if (d2 <= top.worst() && d2 < r2 && p != own && (unsigned)(p - wlo) >= (unsigned)wn) top.offer(d2, r.id);
     }
   };
   int cur = tv.root, visits = 0;

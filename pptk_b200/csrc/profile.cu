@@ -16,6 +16,7 @@ namespace pptkg {
 std::atomic<long long> g_launches{0};
 std::atomic<int> g_tune_lane_span{256};
 std::atomic<int> g_tune_rnear_warp_queries{262144};
+std::atomic<int> g_tune_warm_bound{1};
 thread_local int* g_status_sink = nullptr;
 
 namespace {
@@ -252,6 +253,11 @@ int pptkg_tune_set(const char* name, int64_t value) {
     pptkg::g_tune_rnear_warp_queries.store((int)value);
     return PPTKG_OK;
   }
+  if (std::string(name) == "warm_bound") {
+    if (value < 0 || value > 1) return PPTKG_E_INVALID;
+    pptkg::g_tune_warm_bound.store((int)value);
+    return PPTKG_OK;
+  }
   return PPTKG_E_INVALID;
 }
 
@@ -268,6 +274,10 @@ int pptkg_tune_get(const char* name, int64_t* value) {
   }
   if (std::string(name) == "rnear_warp_queries") {
     *value = pptkg::g_tune_rnear_warp_queries.load();
+    return PPTKG_OK;
+  }
+  if (std::string(name) == "warm_bound") {
+    *value = pptkg::g_tune_warm_bound.load();
     return PPTKG_OK;
   }
   return PPTKG_E_INVALID;

@@ -229,24 +229,75 @@ __device__ __forceinline__ float seed_bound32(const TreeView<T, D>& tv, const fl
   return r;
 }
 
-// Seeds a query's top-k bound from its neighbourhood in tree order.  Keeps a
-// warp of far-apart queries from visiting most of the tree before each
-// query's list fills up.
+// Warm start of a query's top-k list from its neighbourhood in tree order:
+// the list is filled with the candidates at the w tree positions around the
+// query's anchor (w = k, plus one for a self query, whose own position is
+// dropped), sorted, and those positions [wlo, wlo + wn) are skipped by the
+// walk, so every candidate is still offered exactly once.  The list's bound
+// starts at a real k-th distance instead of the radius, which keeps a warp
+// of far-apart queries from visiting most of the tree and means that most
+// candidates the walk meets are rejected without an insertion.
+//
+// Slot j of the window gets: a real key (distance < r2), an empty key (no
+// candidate: outside the tree, or beyond r2), or a dead key (j >= w, or the
+// own position when w = k + 1) -- exactly k live (real or empty) keys, which
+// the descending sort moves to the k live slots of the list.
+//
+// With g_tune_warm_bound, the bound is then lowered to seed_bound32 /
+// seed_bound over a wider window (live keys above it become seed keys);
+// candidates of the wider window outside [wlo, wlo + wn) are offered by the
+// walk as any other.
 template <typename T, int D, typename DistT, typename Top>
-__device__ __forceinline__ void seed_topk(Top& top, const TreeView<T, D>& tv, const SlotMap& fm, int slot,
-                                          const DistT* q, int anchor, int k, int own, DistT r2) {
+__device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, const SlotMap& fm, int slot,
+                                          const DistT* q, int anchor, int k, int own, DistT r2, bool bound,
+                                          int& wlo, int& wn) {
+  constexpr int CAP = Top::CAP;
+  wlo = 0;
+  wn = 0;
+  if (anchor < 0) return;
   int lo = 0, hi = tv.nv;
   if (fm.warp_cloud && !fm.views) {
     const int c = fm.warp_cloud[slot >> 5];
     lo = (int)fm.valid_off[c];
     hi = (int)fm.valid_off[c + 1];
   }
-  DistT b;
-  if constexpr (std::is_same<DistT, float>::value)
-    b = k <= 16 ? seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi) : seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
-  else
-    b = seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
-  top.seed(k, b, r2);
+  if (hi <= lo) return;
+  const int w = min(k + (own >= 0 ? 1 : 0), CAP);
+  const int a = min(max(anchor, lo), hi - 1);
+  const int start = hi - lo >= w ? min(max(a - w / 2, lo), hi - w) : lo;
+#pragma unroll
+  for (int j = 0; j < CAP; j++) {
+    const int p = start + j;
+    if (j >= w) {
+      top.set_dead(j);
+    } else if (p >= hi) {
+      top.set_empty(j);
+    } else if (p == own) {
+      if (w == k + 1)
+        top.set_dead(j);
+      else
+        top.set_empty(j);
+    } else {
+      const PointRec<T, D> r = tv.pts[p];
+      const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
+      if (d2 < r2)
+        top.set_real(j, d2, r.id);
+      else
+        top.set_empty(j);
+    }
+  }
+  top.sort_desc();
+  wlo = start;
+  wn = min(w, hi - start);
+  if (bound) {
+    DistT b;
+    if constexpr (std::is_same<DistT, float>::value)
+      b = k <= 16 ? seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi)
+                  : seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
+    else
+      b = seed_bound<T, D, DistT>(tv, q, anchor, k, own, lo, hi);
+    top.seed(k, b, r2);
+  }
 }
 
 // order_mode 0: slot = query; 1: order[slot]; 2: tree order (query = the
@@ -384,7 +435,8 @@ constexpr int knn_min_blocks(int kmax, int dist_bytes) { return (dist_bytes == 4
 template <typename T, int D, int KMAX, typename L>
 __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename DistOf<T>::type))) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
                                                   int k, typename DistOf<T>::type r2, int32_t* out_idx,
-                                                  int32_t* out_cnt, int* status, SlotMap fm, int lane_span) {
+                                                  int32_t* out_cnt, int* status, SlotMap fm, int lane_span,
+                                                  bool warm_bound) {
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
@@ -404,10 +456,11 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
     for (int d = 0; d < D; d++) q[d] = (DistT)0;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (active) seed_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2);
+  int wlo = 0, wn = 0;
+  if (active) warm_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
   const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
-                      ? lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top)
-                      : packet_knn<T, D>(tv, q, own, active, r2, top, ws);
+                      ? lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top, wlo, wn)
+                      : packet_knn<T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
   if (!ok) atomicExch(status, 1);
   if (qid >= 0) {
     int c = 0;
@@ -432,7 +485,8 @@ void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int 
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
                                                                       d_idx, d_cnt, status, fm,
-                                                                      g_tune_lane_span.load());
+                                                                      g_tune_lane_span.load(),
+                                                                      g_tune_warm_bound.load() != 0);
   PPTKG_CHECK_LAUNCH();
 }
 
@@ -984,7 +1038,8 @@ __global__ void __launch_bounds__(QTHREADS, normals_min_blocks(KMAX, sizeof(type
 k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
-                                                      int* fix, int* nfix, int* status, SlotMap fm, int lane_span) {
+                                                      int* fix, int* nfix, int* status, SlotMap fm, int lane_span,
+                                                      bool warm_bound) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
@@ -1006,10 +1061,11 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   int* lane_log = ws.log + lane;
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
-  if (active) seed_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2);
+  int wlo = 0, wn = 0;
+  if (active) warm_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
   const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
-                      ? lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top)
-                      : packet_knn<T, 3>(tv, q, own, active, r2, top, ws);
+                      ? lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top, wlo, wn)
+                      : packet_knn<T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
   if (!ok) atomicExch(status, 1);
   if (qid < 0) return;
   if (!active) {
@@ -1233,7 +1289,7 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
       view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm,
-      g_tune_lane_span.load());
+      g_tune_lane_span.load(), g_tune_warm_bound.load() != 0);
   PPTKG_CHECK_LAUNCH();
 }
 

@@ -65,8 +65,11 @@ def _run_both(tree, idx, m, k, prec, tdt, calls=2):
     ev = torch.empty((m, 3, 3), device="cuda", dtype=tdt)
     ew = torch.empty((m, 3), device="cuda", dtype=tdt)
     sz = torch.empty((m,), device="cuda", dtype=torch.int32)
-    N.call("pptkg_tree_normals", tree._h, iptr, m, N.MEM_DEVICE, k, ctypes.c_float(np.inf), 3, prec, N.ptr(ev),
-           N.ptr(ew), N.ptr(sz), stream)
+    # the allocating entry reads NULL indices as all rows, so the first m
+    # rows are passed to it explicitly
+    rows = idx if idx is not None else torch.arange(m, device="cuda", dtype=torch.int32)
+    N.call("pptkg_tree_normals", tree._h, N.ptr(rows), m, N.MEM_DEVICE, k, ctypes.c_float(np.inf), 3, prec,
+           N.ptr(ev), N.ptr(ew), N.ptr(sz), stream)
     ref = [x.cpu().numpy() for x in (ev, ew, sz)]
     got = []
     for _ in range(calls):
