@@ -229,13 +229,15 @@ class Server:
         transient needs of admitted requests.
     slots: batches that may run at once, each on its own CUDA stream.  The
         last `fast_slots` of them run on high-priority streams and serve
-        small requests only (at most `small_batch` queries each), so that a
-        small request never waits behind the rows of a large one.
-    batch_ms: time budget of one batch.  The queries folded into a batch are
-        capped at the measured rate (queries per second of recent batches)
-        times this budget, within [min_batch_queries, max_batch_queries];
-        a request larger than the cap is answered in slices of the cap, so
-        requests submitted after it interleave with its slices.
+        small requests only (at most `small_batch` queries each), taken from
+        anywhere in the queue, so that a small request never waits behind a
+        large one.
+    max_batch_queries: upper bound on the queries folded into one batch; a
+        request larger than the cap runs in cap-sized slices, so requests
+        submitted after it interleave with its slices.
+    batch_ms: optional time budget of one batch: the cap becomes the measured
+        rate (queries per second of recent batches) times this budget, within
+        [min_batch_queries, max_batch_queries].
     max_host_batch_queries: the upper bound for batches that return numpy
         results: smaller batches let one batch's host copies overlap another
         batch's kernels.
@@ -244,9 +246,8 @@ class Server:
         and after its work (``trace`` list of (kinds, fast slot, start,
         end)), so that the device-side overlap of batches can be checked.
 
-    Requests are admitted first-in first-out within each of two queues
-    (small requests, and everything else) against the HBM budget; a
-    request's Future may be cancelled (``future.cancel()``) until its last
+    Requests are admitted first-in first-out (the fast slots excepted)
+    against the HBM budget; a request's Future may be cancelled (``future.cancel()``) until its last
     rows are answered: rows not yet started are never run, and the answer of
     rows in flight is discarded.  A batch that fails fails the requests it
     held rows of; the server keeps serving.
@@ -267,8 +268,7 @@ class Server:
         self.trees = {}
         self.tree_bytes = {}
         self._next_id = 0
-        self._small = deque()
-        self._large = deque()
+        self._queue = deque()
         self._committed = 0.0
         self._cv = threading.Condition()
         fast_slots = max(0, min(int(fast_slots), slots - 1))
@@ -345,8 +345,7 @@ class Server:
         with self._cv:
             if not self._running:
                 raise RuntimeError("server closed")
-            small = r.kind in ("knn", "normals", "rnear") and r.m <= self.small_batch
-            (self._small if small else self._large).append(r)
+            self._queue.append(r)
             self._cv.notify_all()
         return r.future
 
@@ -359,41 +358,41 @@ class Server:
         return int(min(top, max(self.min_batch, self._rate * self.batch_ms / 1e3)))
 
     def _admit(self, fast):
-        """Slices of requests for the next batch, first-in first-out within a
-        queue under the budget.  A fast slot takes small requests only, up to
-        small_batch queries; another slot takes the large queue first.  A
-        build or r-near request runs as a batch of its own; kNN and normal
-        rows are folded up to the batch cap, the last request possibly cut."""
-        queues = [self._small] if fast else [self._large, self._small]
-        for q in queues:
-            out = self._admit_from(q, self.small_batch if fast else None)
-            if out:
-                return out
-        return []
+        """Slices of requests for the next batch, under the HBM budget.
 
-    def _admit_from(self, q, limit):
+        A normal slot takes requests first-in first-out from the head of
+        the queue and folds kNN / normal requests up to the batch cap; a
+        request never straddles two batches unless it is larger than the cap
+        by itself, in which case it runs in cap-sized slices, one batch each.
+        A fast slot takes small requests (at most small_batch queries) from
+        anywhere in the queue, oldest first, up to small_batch queries in
+        all, so that a small request never waits behind a large one.  A
+        build or r-near request runs as a batch of its own."""
         out = []
         queries = 0
         host = False
-        while q:
-            r = q[0]
+        q = self._queue
+        i = 0
+        while i < len(q):
+            r = q[i]
             if r.future.done():  # cancelled (or failed) while queued: its rows
-                q.popleft()      # not yet admitted never run (nothing of them was committed)
+                del q[i]         # not yet admitted never run (nothing of them was committed)
                 continue
             if r.kind != "build" and r.args[0] not in self.trees:
-                q.popleft()
+                del q[i]
                 r.future.set_exception(KeyError(f"unknown tree {r.args[0]}"))
+                continue
+            small = r.kind != "build" and r.m <= self.small_batch and r.next_row == 0
+            if fast and not small:
+                i += 1
                 continue
             exclusive = r.kind in ("build", "rnear")
             r_host = bool(r.key and r.key[-1] is True)
-            cap = self.batch_cap(host or r_host)
-            if limit is not None:
-                cap = min(cap, limit)
-            if out and (exclusive or queries >= cap):
+            cap = min(self.batch_cap(host or r_host), self.small_batch) if fast else self.batch_cap(host or r_host)
+            left = r.m - r.next_row
+            if out and (exclusive or queries + left > cap):
                 break
-            take = r.m - r.next_row if exclusive else min(r.m - r.next_row, max(cap - queries, 0))
-            if take <= 0 and r.m > 0:
-                break
+            take = left if (exclusive or left <= cap) else cap
             part = r.bytes * take / max(r.m, 1) if r.m else r.bytes
             if self._committed + part > self.budget:
                 break
@@ -405,7 +404,9 @@ class Server:
             queries += take
             host = host or r_host
             if r.next_row >= r.m:
-                q.popleft()
+                del q[i]
+            else:
+                break  # a slice of a large request is a batch of its own
             if exclusive:
                 break
         return out
@@ -413,9 +414,9 @@ class Server:
     def _loop(self):
         while True:
             with self._cv:
-                while self._running and (not (self._small or self._large) or not self._free):
+                while self._running and (not self._queue or not self._free):
                     self._cv.wait(0.01)
-                if not self._running and not (self._small or self._large):
+                if not self._running and not self._queue:
                     return
                 if not self._free:
                     continue
@@ -535,11 +536,10 @@ class Server:
         RuntimeError, running batches finish."""
         with self._cv:
             self._running = False
-            for q in (self._small, self._large):
-                while q:
-                    r = q.popleft()
-                    if not r.future.done():
-                        r.future.set_exception(RuntimeError("server closed"))
+            while self._queue:
+                r = self._queue.popleft()
+                if not r.future.done():
+                    r.future.set_exception(RuntimeError("server closed"))
             self._cv.notify_all()
         self._thread.join()
         self._pool.shutdown(wait=True)
