@@ -442,7 +442,7 @@ def run_ragged_workload(args, ctx):
     """Ragged batch: 4,096 clouds (synth.ragged_clouds, seed 4, sizes
     log-uniform in [1k, 200k]); one step builds every cloud's tree in one
     forest build and answers kNN k=16 and normals k=16 for every point of
-    every cloud.  Bucket size and lane_span are picked by the autotuner on
+    every cloud.  Bucket size, lane_span, warm_bound and topk_min are picked by the autotuner on
     the first 256 clouds before timing."""
     torch = ctx.torch
     from pptk_b200 import autotune, ragged, synth
@@ -501,7 +501,9 @@ def run_ragged_workload(args, ctx):
                        "clouds": 4096, "points": n, "k": k, "l2": f"inputs ({P.nbytes / 1e9:.2f} GB) larger than L2",
                        "parallelism": f"replicas x{ctx.world}"},
             "autotune": {"bucket": tuned["bucket"], "lane_span": tuned["lane_span"],
-                         "sample": "first 256 clouds", "table": tuned["table"]},
+                         "warm_bound": tuned.get("warm_bound"), "topk_min": tuned.get("topk_min"),
+                         "sample": "first 256 clouds", "table": tuned["table"],
+                         "knob_table": tuned.get("knob_table")},
             "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
                              "ms_per_step": ms_q, "what": "kNN + normals of every point, replayed from two CUDA "
                                                          "graphs on the built forest"},

@@ -264,7 +264,9 @@ PPTKG_API int64_t pptkg_launch_count(void);
  * pptk_b200/autotune.py).  Settings are process-wide and read at launch.
  *   "lane_span": a kNN / normals warp whose 32 queries span more than this
  *     many tree positions walks the tree per lane rather than as one packet
- *     (-1: always packets).  Default 256.
+ *     (-1: always packets).  Default 1024 (with warm-started lists, packets
+ *     won down to about one query per ten tree points: 2M random queries on
+ *     a 20M-point scene took 6.3 ms as packets, 10.6-12.0 ms with 256).
  *   "rnear_warp_queries": pptkg_rnear_count / pptkg_rnear_fill calls, and
  *     normals over r-near neighbourhoods (k = -1), with at most this many
  *     queries give each query a whole warp (the lanes split every bucket)
@@ -277,6 +279,9 @@ PPTKG_API int64_t pptkg_launch_count(void);
  *     k-th distance over a wider window of tree-order neighbours (fewer
  *     list insertions), with 0 not.  Default 1.  Results do not depend on
  *     it.
+ *   "topk_min": the k-tiling of the register top-k lists: 0 (default) uses
+ *     the smallest capacity of 4, 8, 16, 32, 64 that holds k; 4 ... 64 use at
+ *     least that capacity.  Results do not depend on it.
  * Unknown names or out-of-range values: PPTKG_E_INVALID. */
 PPTKG_API int pptkg_tune_set(const char* name, int64_t value);
 PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);

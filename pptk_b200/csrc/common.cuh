@@ -55,6 +55,10 @@ extern std::atomic<int> g_tune_rnear_warp_queries;
 //    the k-th distance of the 32 (k <= 16) or 3 x k tree-order neighbours
 //    of the query's anchor (1) or not (0).
 extern std::atomic<int> g_tune_warm_bound;
+//  topk_min: smallest top-k list capacity used (0: the smallest of 4, 8, 16,
+//    32, 64 that holds k; otherwise at least this one) -- the k-tiling of the
+//    register lists.
+extern std::atomic<int> g_tune_topk_min;
 
 // Status sink of this host thread (pptkg_set_status_sink): while set, query
 // entry points record kernel check failures into this device word and

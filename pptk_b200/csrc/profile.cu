@@ -14,9 +14,10 @@
 namespace pptkg {
 
 std::atomic<long long> g_launches{0};
-std::atomic<int> g_tune_lane_span{256};
+std::atomic<int> g_tune_lane_span{1024};
 std::atomic<int> g_tune_rnear_warp_queries{262144};
 std::atomic<int> g_tune_warm_bound{1};
+std::atomic<int> g_tune_topk_min{0};
 thread_local int* g_status_sink = nullptr;
 
 namespace {
@@ -258,6 +259,11 @@ int pptkg_tune_set(const char* name, int64_t value) {
     pptkg::g_tune_warm_bound.store((int)value);
     return PPTKG_OK;
   }
+  if (std::string(name) == "topk_min") {
+    if (value != 0 && value != 4 && value != 8 && value != 16 && value != 32 && value != 64) return PPTKG_E_INVALID;
+    pptkg::g_tune_topk_min.store((int)value);
+    return PPTKG_OK;
+  }
   return PPTKG_E_INVALID;
 }
 
@@ -278,6 +284,10 @@ int pptkg_tune_get(const char* name, int64_t* value) {
   }
   if (std::string(name) == "warm_bound") {
     *value = pptkg::g_tune_warm_bound.load();
+    return PPTKG_OK;
+  }
+  if (std::string(name) == "topk_min") {
+    *value = pptkg::g_tune_topk_min.load();
     return PPTKG_OK;
   }
   return PPTKG_E_INVALID;

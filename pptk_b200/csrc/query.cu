@@ -493,13 +493,14 @@ void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int 
 template <typename T, int D, typename L>
 void dispatch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                   int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm = SlotMap{}) {
-  if (k <= 4)
+  const int kc = std::max(k, g_tune_topk_min.load());
+  if (kc <= 4)
     launch_knn<T, D, 4>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
-  else if (k <= 8)
+  else if (kc <= 8)
     launch_knn<T, D, 8>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
-  else if (k <= 16)
+  else if (kc <= 16)
     launch_knn<T, D, 16>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
-  else if (k <= 32)
+  else if (kc <= 32)
     launch_knn<T, D, 32>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
   else
     launch_knn<T, D, 64>(t, ld, order, mode, m, k, r2, d_idx, d_cnt, status, st, fm);
@@ -1320,13 +1321,14 @@ template <typename T, typename L>
 void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k,
                       typename DistOf<T>::type r2, int num_eigen, int prec, double gap_thr, T* ev, T* ew,
                       int32_t* sz, int* status, cudaStream_t st, SlotMap fm = SlotMap{}) {
-  if (k <= 4)
+  const int kc = std::max(k, g_tune_topk_min.load());
+  if (kc <= 4)
     normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
-  else if (k <= 8)
+  else if (kc <= 8)
     normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
-  else if (k <= 16)
+  else if (kc <= 16)
     normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
-  else if (k <= 32)
+  else if (kc <= 32)
     normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
   else
     normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);

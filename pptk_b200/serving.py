@@ -254,7 +254,7 @@ class Server:
     """
 
     def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=20_000_000, engine=None,
-                 fast_slots=1, small_batch=1_000_000, max_host_batch_queries=8_000_000, batch_ms=None,
+                 fast_slots=1, small_batch=65_536, max_host_batch_queries=8_000_000, batch_ms=None,
                  min_batch_queries=1_000_000, trace=False):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)

@@ -46,8 +46,10 @@ def test_tuning_knobs_validate_and_round_trip():
     # process-wide traversal knobs: defaults, accepted ranges, rejected values
     from pptk_b200 import _native as N
     lib = N.lib()
-    for name, default, good, bad in (("lane_span", 256, (-1, 0, 64, 1 << 20), (-2,)),
-                                     ("rnear_warp_queries", 262144, (0, 1, 1 << 30), (-1,))):
+    for name, default, good, bad in (("lane_span", 1024, (-1, 0, 64, 1 << 20), (-2,)),
+                                     ("rnear_warp_queries", 262144, (0, 1, 1 << 30), (-1,)),
+                                     ("warm_bound", 1, (0, 1), (-1, 2)),
+                                     ("topk_min", 0, (4, 8, 16, 32, 64, 0), (-1, 3, 65, 128))):
         assert N.tune_get(name) == default
         try:
             for v in good:
