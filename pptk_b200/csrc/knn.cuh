@@ -70,6 +70,29 @@ __device__ __forceinline__ DistT box_max_dist2(const T* lo, const T* hi, const D
 template <int KMAX, typename DistT>
 struct TopK;
 
+// Bitonic sort of N 64-bit keys held in registers (fully unrolled), into
+// descending (desc = true) or ascending order.
+template <int N>
+__device__ __forceinline__ void bitonic_sort(unsigned long long (&a)[N], bool desc) {
+#pragma unroll
+  for (int size = 2; size <= N; size <<= 1)
+#pragma unroll
+    for (int stride = size / 2; stride > 0; stride >>= 1)
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const unsigned long long x = a[i], y = a[j];
+          // blocks alternate direction; the last stage (size == N) has the
+          // requested one
+          const bool up = ((i & size) != 0) == desc;
+          const bool sw = up ? (x > y) : (x < y);
+          a[i] = sw ? y : x;
+          a[j] = sw ? x : y;
+        }
+      }
+}
+
 // float distances: (dist2 bits << 32 | id) packed into one 64-bit key;
 // non-negative floats order like their bit patterns.
 template <int KMAX>
@@ -120,24 +143,30 @@ struct TopK<KMAX, float> {
   }
   __device__ __forceinline__ void set_empty(int j) { s[j] = lim; }
   __device__ __forceinline__ void set_dead(int j) { s[j] = 0ull; }
-  __device__ __forceinline__ void sort_desc() {
-    // bitonic network, fully unrolled over the compile-time capacity
+  __device__ __forceinline__ void sort_desc() { bitonic_sort<KMAX>(s, true); }
+  // The KMAX smallest of this list (sorted descending) and t (KMAX keys
+  // sorted ascending), sorted descending: the element-wise minimum of the
+  // two is a bitonic sequence holding them, and a bitonic merge sorts it.
+  __device__ __forceinline__ void merge_smallest(const unsigned long long (&t)[KMAX]) {
 #pragma unroll
-    for (int size = 2; size <= KMAX; size <<= 1)
+    for (int j = 0; j < KMAX; j++) s[j] = t[j] < s[j] ? t[j] : s[j];
 #pragma unroll
-      for (int stride = size / 2; stride > 0; stride >>= 1)
+    for (int stride = KMAX / 2; stride > 0; stride >>= 1)
 #pragma unroll
-        for (int i = 0; i < KMAX; i++) {
-          const int j = i ^ stride;
-          if (j > i) {
-            const unsigned long long a = s[i], b = s[j];
-            const bool up = (i & size) != 0;  // this block ends ascending
-            const bool sw = up ? (a > b) : (a < b);
-            s[i] = sw ? b : a;
-            s[j] = sw ? a : b;
-          }
+      for (int i = 0; i < KMAX; i++) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const unsigned long long x = s[i], y = s[j];
+          const bool sw = x < y;
+          s[i] = sw ? y : x;
+          s[j] = sw ? x : y;
         }
+      }
   }
+  __device__ __forceinline__ unsigned long long key_real(float d2, int id) const {
+    return ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
+  }
+  __device__ __forceinline__ unsigned long long key_empty() const { return lim; }
 };
 
 // double distances: parallel (dist2, id) arrays compared lexicographically.

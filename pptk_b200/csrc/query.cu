@@ -247,6 +247,10 @@ __device__ __forceinline__ float seed_bound32(const TreeView<T, D>& tv, const fl
 // seed_bound over a wider window (live keys above it become seed keys);
 // candidates of the wider window outside [wlo, wlo + wn) are offered by the
 // walk as any other.
+//
+// Float lists with k equal to their capacity (k = 4, 8, 16) start from a
+// window of 2k positions instead: the list then holds the k nearest of 2k
+// tree-order neighbours, all of them real candidates.
 template <typename T, int D, typename DistT, typename Top>
 __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, const SlotMap& fm, int slot,
                                           const DistT* q, int anchor, int k, int own, DistT r2, bool bound,
@@ -262,6 +266,41 @@ __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, co
     hi = (int)fm.valid_off[c + 1];
   }
   if (hi <= lo) return;
+  if constexpr (std::is_same<DistT, float>::value && CAP <= 16) {
+    if (k == CAP) {
+      // twice as wide a window: its first CAP keys fill the list, the
+      // others are sorted apart and merged in, so the list holds the CAP
+      // nearest of 2 CAP tree-order neighbours (all real unless the window
+      // is short) and its bound is their CAP-th distance
+      constexpr int W = 2 * CAP;
+      const int a2 = min(max(anchor, lo), hi - 1);
+      const int start = hi - lo >= W ? min(max(a2 - CAP, lo), hi - W) : lo;
+      unsigned long long t[CAP];
+#pragma unroll
+      for (int j = 0; j < W; j++) {
+        const int p = start + j;
+        unsigned long long key = top.key_empty();
+        if (p < hi && p != own) {
+          const PointRec<T, D> r = tv.pts[p];
+          const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
+          if (d2 < r2) key = top.key_real(d2, r.id);
+        }
+        if (j < CAP)
+          top.s[j] = key;
+        else
+          t[j - CAP] = key;
+      }
+      top.sort_desc();
+      bitonic_sort<CAP>(t, false);
+      top.merge_smallest(t);
+      wlo = start;
+      wn = min(W, hi - start);
+      // with CAP = 16 the window is seed_bound32's own: its bound is the
+      // list's already
+      if (bound && CAP < 16) top.seed(k, seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi), r2);
+      return;
+    }
+  }
   const int w = min(k + (own >= 0 ? 1 : 0), CAP);
   const int a = min(max(anchor, lo), hi - 1);
   const int start = hi - lo >= w ? min(max(a - w / 2, lo), hi - w) : lo;
