@@ -31,8 +31,10 @@ TreeView<T, D> view_of(const TreeBase* t) {
 }
 
 // Per-warp shared memory: the staging buffer (a leaf chunk in r-near walks,
-// the warp's queries in kNN walks), traversal stack, the 32 x 33 distance
-// matrix and the 32 candidate ids of the kNN bucket scan, and (normals)
+// the warp's queries in kNN walks), traversal stack, then either the 32 x 33
+// distance matrix and the 32 candidate ids of the register-list kNN scan, or
+// (coop = the list capacity, packet_knn_coop) the 32 shared lists, the
+// candidate keys of one step and the queries' exclusions; and (normals)
 // `logcap` list slots per lane.
 template <typename T, int D>
 __host__ __device__ constexpr size_t stage_bytes() {
@@ -40,30 +42,56 @@ __host__ __device__ constexpr size_t stage_bytes() {
   return 32 * (sizeof(PointRec<T, D>) > sizeof(QStage<DistT, D>) ? sizeof(PointRec<T, D>) : sizeof(QStage<DistT, D>));
 }
 
-template <typename T, int D>
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
-  typedef typename DistOf<T>::type DistT;
-  return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
-         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4 + (size_t)logcap * 32 * 4;
+__host__ __device__ constexpr size_t coop_bytes(int coop) {
+  return coop ? (size_t)32 * (coop + 1) * 8 + (size_t)(32 / coop) * 32 * 8 + 32 * 16 : 0;
 }
 
 template <typename T, int D>
-__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0) {
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0, int coop = 0) {
+  typedef typename DistOf<T>::type DistT;
+  const size_t lists = coop ? coop_bytes(coop) : ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4;
+  return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) + lists +
+         (size_t)logcap * 32 * 4;
+}
+
+template <typename T, int D>
+__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0, int coop = 0) {
   typedef typename DistOf<T>::type DistT;
   extern __shared__ __align__(16) unsigned char qsm[];
-  const size_t per = warp_smem_bytes<T, D>(depth, logcap);
+  const size_t per = warp_smem_bytes<T, D>(depth, logcap, coop);
   unsigned char* base = qsm + (threadIdx.x >> 5) * per;
   WarpScratch<T, D> ws;
   ws.buf = (PointRec<T, D>*)base;
   base += stage_bytes<T, D>();
   ws.stack = (int*)base;
   base += ((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15;
-  ws.dmat = (DistT*)base;
-  base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
-  ws.cid = (int*)base;
-  base += 32 * 4;
+  ws.dmat = nullptr;
+  ws.cid = nullptr;
+  ws.rows = nullptr;
+  ws.kst = nullptr;
+  ws.excl = nullptr;
+  if (coop) {
+    ws.rows = (unsigned long long*)base;
+    base += (size_t)32 * (coop + 1) * 8;
+    ws.kst = (unsigned long long*)base;
+    base += (size_t)(32 / coop) * 32 * 8;
+    ws.excl = (int4*)base;
+    base += 32 * 16;
+  } else {
+    ws.dmat = (DistT*)base;
+    base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
+    ws.cid = (int*)base;
+    base += 32 * 4;
+  }
   ws.log = logcap ? (int*)base : nullptr;
   return ws;
+}
+
+// The list capacity whose packet walks use cooperative shared-memory lists
+// (packet_knn_coop), or 0: float distances and capacities up to 32.
+template <typename T, int KMAX>
+__host__ __device__ constexpr int coop_kmax() {
+  return (std::is_same<typename DistOf<T>::type, float>::value && KMAX <= 32) ? KMAX : 0;
 }
 
 // Candidate-log capacity per lane of the normals kernel.
@@ -479,7 +507,8 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
+  constexpr int COOP = coop_kmax<T, KMAX>();
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth, 0, COOP);
   int qid = -1, own = -1, anchor = -1;
   DistT q[D];
   bool active = false;
@@ -497,9 +526,15 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
   top.reset(k, r2);
   int wlo = 0, wn = 0;
   if (active) warm_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
-  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
-                      ? lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top, wlo, wn)
-                      : packet_knn<T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
+  bool ok;
+  if (use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)) {
+    ok = lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top, wlo, wn);
+  } else {
+    if constexpr (COOP > 0)
+      ok = packet_knn_coop<KMAX, T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
+    else
+      ok = packet_knn<T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
+  }
   if (!ok) atomicExch(status, 1);
   if (qid >= 0) {
     int c = 0;
@@ -519,7 +554,7 @@ template <typename T, int D, int KMAX, typename L>
 void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                 int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth, 0, coop_kmax<T, KMAX>());
   if (smem > 48 * 1024)
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
@@ -1082,9 +1117,10 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       bool warm_bound) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
+  constexpr int COOP = coop_kmax<T, KMAX>();
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP, COOP);
   const int lane = threadIdx.x & 31;
   int qid = -1, own = -1, grp = 0, anchor = -1;
   DistT q[3];
@@ -1103,9 +1139,15 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   top.reset(k, r2);
   int wlo = 0, wn = 0;
   if (active) warm_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
-  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
-                      ? lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top, wlo, wn)
-                      : packet_knn<T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
+  bool ok;
+  if (use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)) {
+    ok = lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top, wlo, wn);
+  } else {
+    if constexpr (COOP > 0)
+      ok = packet_knn_coop<KMAX, T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
+    else
+      ok = packet_knn<T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
+  }
   if (!ok) atomicExch(status, 1);
   if (qid < 0) return;
   if (!active) {
@@ -1323,7 +1365,7 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
                     cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
+  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX), coop_kmax<T, KMAX>());
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
