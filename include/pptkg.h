@@ -279,6 +279,10 @@ PPTKG_API int64_t pptkg_launch_count(void);
  *     k-th distance over a wider window of tree-order neighbours (fewer
  *     list insertions), with 0 not.  Default 1.  Results do not depend on
  *     it.
+ *   "warm_mult": float lists whose k equals their capacity (4, 8, 16, 32)
+ *     start from the k nearest of warm_mult x k tree-order neighbours of the
+ *     query's anchor (1 to 8; 1 gives the k-position start).  Default 2.
+ *     Results do not depend on it.
  *   "topk_min": the k-tiling of the register top-k lists: 0 (default) uses
  *     the smallest capacity of 4, 8, 16, 32, 64 that holds k; 4 ... 64 use at
  *     least that capacity.  Results do not depend on it.

@@ -59,6 +59,9 @@ extern std::atomic<int> g_tune_warm_bound;
 //    32, 64 that holds k; otherwise at least this one) -- the k-tiling of the
 //    register lists.
 extern std::atomic<int> g_tune_topk_min;
+//  warm_mult: float lists whose k equals their capacity start warm from the
+//    k nearest of warm_mult x k tree-order neighbours (1: from k of them).
+extern std::atomic<int> g_tune_warm_mult;
 
 // Status sink of this host thread (pptkg_set_status_sink): while set, query
 // entry points record kernel check failures into this device word and

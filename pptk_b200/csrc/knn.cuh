@@ -144,12 +144,15 @@ struct TopK<KMAX, float> {
   __device__ __forceinline__ void set_empty(int j) { s[j] = lim; }
   __device__ __forceinline__ void set_dead(int j) { s[j] = 0ull; }
   __device__ __forceinline__ void sort_desc() { bitonic_sort<KMAX>(s, true); }
-  // The KMAX smallest of this list (sorted descending) and t (KMAX keys
-  // sorted ascending), sorted descending: the element-wise minimum of the
-  // two is a bitonic sequence holding them, and a bitonic merge sorts it.
-  __device__ __forceinline__ void merge_smallest(const unsigned long long (&t)[KMAX]) {
+  // The KMAX smallest of this list (sorted descending) and t (Q <= KMAX
+  // keys sorted ascending, read as padded with keys above every list key),
+  // sorted descending: the element-wise minimum of the two is a bitonic
+  // sequence holding them, and a bitonic merge sorts it.
+  template <int Q>
+  __device__ __forceinline__ void merge_smallest(const unsigned long long (&t)[Q]) {
+    static_assert(Q <= KMAX, "merge of at most KMAX keys");
 #pragma unroll
-    for (int j = 0; j < KMAX; j++) s[j] = t[j] < s[j] ? t[j] : s[j];
+    for (int j = 0; j < Q; j++) s[j] = t[j] < s[j] ? t[j] : s[j];
 #pragma unroll
     for (int stride = KMAX / 2; stride > 0; stride >>= 1)
 #pragma unroll
@@ -261,10 +264,6 @@ struct WarpScratch {
   int* log;                              // per-lane neighbour lists, lane-strided; null when unused
   typename DistOf<T>::type* dmat;        // 32 x 33 distances (kNN bucket scan); null when unused
   int* cid;                              // 32 candidate ids of the chunk being scanned (kNN)
-  // cooperative float lists (packet_knn_coop); null when unused
-  unsigned long long* rows;              // 32 rows of KMAX + 1 keys
-  unsigned long long* kst;               // candidate keys of one step, 32 per lane group
-  int4* excl;                            // per query: warm window start, length, own position
 };
 
 // A lane's query as the rest of its warp reads it during a bucket scan:
@@ -503,114 +502,6 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
     }
   };
   return packet_walk<T, D, DistT>(tv, q, active, ws, need, scan);
-}
-
-// The same kNN with the warp's 32 float lists in shared memory, each list
-// held by KMAX cooperating lanes (KMAX <= 32): 32 / KMAX lists take one
-// candidate each per step.  Lane j of a group holds slot j of the list
-// (descending, slot 0 the current k-th); a candidate's insertion point is
-// the ballot count of the slots above it, and the slots above that point
-// shift down by one with a shuffle.  Inserting is thus a few warp
-// instructions for every lane that has a candidate, instead of a
-// KMAX-wide compare network run by one lane while the lanes without a
-// candidate wait.  The list (warm-started in registers) moves to shared
-// memory for the walk and back afterwards; the result is identical to
-// packet_knn's.
-//
-// Shared memory per warp (ws.rows etc.): rows[32][KMAX + 1] keys, the
-// candidate keys of the current step kst[32 / KMAX][32], and per query its
-// coordinates and entry bound (ws.buf, QStage) and its exclusions
-// (ws.excl: warm window start, length, own position).
-template <int KMAX, typename T, int D>
-__device__ bool packet_knn_coop(const TreeView<T, D>& tv, const float* q, int own, bool active, float r2,
-                                TopK<KMAX, float>& top, WarpScratch<T, D> ws, int wlo, int wn) {
-  static_assert(KMAX <= 32 && (32 % KMAX) == 0, "cooperative lists need KMAX | 32");
-  constexpr int G = 32 / KMAX;
-  constexpr int RS = KMAX + 1;  // row stride (keys): rows start in different banks
-  const int lane = threadIdx.x & 31;
-  const unsigned FULL = 0xffffffffu;
-  const int grp = lane / KMAX, slot = lane % KMAX;
-  const unsigned gbits = KMAX == 32 ? FULL : ((1u << KMAX) - 1u);
-  QStage<float, D>* qst = reinterpret_cast<QStage<float, D>*>(ws.buf);
-  int4* xst = ws.excl;
-  unsigned long long* rows = ws.rows;
-  unsigned long long* kst = ws.kst;
-  const float r2_below = below(r2);
-  // the lane's list to its row; its query, bound and exclusions to the stages
-#pragma unroll
-  for (int j = 0; j < KMAX; j++) rows[lane * RS + j] = top.s[j];
-#pragma unroll
-  for (int d = 0; d < D; d++) qst[lane].q[d] = q[d];
-  qst[lane].thr = active ? entry_bound(top.worst(), r2_below) : -1.f;
-  xst[lane] = make_int4(wlo, wn, own, 0);
-  __syncwarp();
-  auto need = [&](float md) { return active && md <= qst[lane].thr; };
-  auto scan = [&](int begin, int count, bool mine) {
-    const unsigned needm = __ballot_sync(FULL, mine);
-    for (int base = begin; base < begin + count; base += 32) {
-      const int nb = min(32, begin + count - base);
-      PointRec<T, D> pr;
-      if (lane < nb) {
-        pr = tv.pts[base + lane];
-      } else {
-#pragma unroll
-        for (int d = 0; d < D; d++) pr.c[d] = (T)0;
-        pr.id = -1;
-      }
-      const int pos = base + lane;
-      unsigned rem = needm;
-      while (rem) {
-        // the next G queries needing this chunk, one per lane group
-        int qi[G];
-        unsigned mk[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-          qi[g] = rem ? __ffs(rem) - 1 : -1;
-          rem &= rem ? rem - 1 : 0u;
-          mk[g] = 0u;
-          if (qi[g] >= 0) {
-            const QStage<float, D> qs = qst[qi[g]];
-            const int4 x = xst[qi[g]];
-            const float d2 = point_dist2<T, float, D>(pr.c, qs.q);
-            const bool excl = (unsigned)(pos - x.x) < (unsigned)x.y || pos == x.z;
-            mk[g] = __ballot_sync(FULL, lane < nb && !excl && d2 <= qs.thr);
-            kst[g * 32 + lane] = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)pr.id;
-          }
-        }
-        int myq = -1;
-        unsigned mym = 0u;
-#pragma unroll
-        for (int g = 0; g < G; g++)
-          if (g == grp) {
-            myq = qi[g];
-            mym = mk[g];
-          }
-        __syncwarp();
-        while (__any_sync(FULL, mym != 0u)) {
-          const int t = mym ? __ffs(mym) - 1 : -1;
-          const bool ins = t >= 0;
-          const unsigned long long c = ins ? kst[grp * 32 + t] : 0ull;
-          const unsigned long long cur = ins ? rows[myq * RS + slot] : 0ull;
-          const unsigned bal = __ballot_sync(FULL, ins && cur > c);
-          const int p = __popc((bal >> (grp * KMAX)) & gbits);
-          const unsigned long long nxt = __shfl_down_sync(FULL, cur, 1, KMAX);
-          if (ins && p > 0) {
-            const unsigned long long nv = slot < p - 1 ? nxt : (slot == p - 1 ? c : cur);
-            rows[myq * RS + slot] = nv;
-            if (slot == 0) qst[myq].thr = entry_bound(__uint_as_float((unsigned)(nv >> 32)), r2_below);
-          }
-          mym &= mym ? mym - 1 : 0u;
-          __syncwarp();
-        }
-      }
-    }
-  };
-  const bool ok = packet_walk<T, D, float>(tv, q, active, ws, need, scan);
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < KMAX; j++) top.s[j] = rows[lane * RS + j];
-  __syncwarp();
-  return ok;
 }
 
 // Per-lane traversal for warps whose queries lie far apart, where a packet

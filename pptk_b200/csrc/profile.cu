@@ -18,6 +18,7 @@ std::atomic<int> g_tune_lane_span{1024};
 std::atomic<int> g_tune_rnear_warp_queries{262144};
 std::atomic<int> g_tune_warm_bound{1};
 std::atomic<int> g_tune_topk_min{0};
+std::atomic<int> g_tune_warm_mult{2};
 thread_local int* g_status_sink = nullptr;
 
 namespace {
@@ -264,6 +265,11 @@ int pptkg_tune_set(const char* name, int64_t value) {
     pptkg::g_tune_topk_min.store((int)value);
     return PPTKG_OK;
   }
+  if (std::string(name) == "warm_mult") {
+    if (value < 1 || value > 8) return PPTKG_E_INVALID;
+    pptkg::g_tune_warm_mult.store((int)value);
+    return PPTKG_OK;
+  }
   return PPTKG_E_INVALID;
 }
 
@@ -288,6 +294,10 @@ int pptkg_tune_get(const char* name, int64_t* value) {
   }
   if (std::string(name) == "topk_min") {
     *value = pptkg::g_tune_topk_min.load();
+    return PPTKG_OK;
+  }
+  if (std::string(name) == "warm_mult") {
+    *value = pptkg::g_tune_warm_mult.load();
     return PPTKG_OK;
   }
   return PPTKG_E_INVALID;

@@ -31,10 +31,8 @@ TreeView<T, D> view_of(const TreeBase* t) {
 }
 
 // Per-warp shared memory: the staging buffer (a leaf chunk in r-near walks,
-// the warp's queries in kNN walks), traversal stack, then either the 32 x 33
-// distance matrix and the 32 candidate ids of the register-list kNN scan, or
-// (coop = the list capacity, packet_knn_coop) the 32 shared lists, the
-// candidate keys of one step and the queries' exclusions; and (normals)
+// the warp's queries in kNN walks), traversal stack, the 32 x 33 distance
+// matrix and the 32 candidate ids of the kNN bucket scan, and (normals)
 // `logcap` list slots per lane.
 template <typename T, int D>
 __host__ __device__ constexpr size_t stage_bytes() {
@@ -42,56 +40,30 @@ __host__ __device__ constexpr size_t stage_bytes() {
   return 32 * (sizeof(PointRec<T, D>) > sizeof(QStage<DistT, D>) ? sizeof(PointRec<T, D>) : sizeof(QStage<DistT, D>));
 }
 
-__host__ __device__ constexpr size_t coop_bytes(int coop) {
-  return coop ? (size_t)32 * (coop + 1) * 8 + (size_t)(32 / coop) * 32 * 8 + 32 * 16 : 0;
-}
-
 template <typename T, int D>
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0, int coop = 0) {
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
-  const size_t lists = coop ? coop_bytes(coop) : ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4;
-  return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) + lists +
-         (size_t)logcap * 32 * 4;
+  return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
+         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4 + (size_t)logcap * 32 * 4;
 }
 
 template <typename T, int D>
-__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0, int coop = 0) {
+__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
   extern __shared__ __align__(16) unsigned char qsm[];
-  const size_t per = warp_smem_bytes<T, D>(depth, logcap, coop);
+  const size_t per = warp_smem_bytes<T, D>(depth, logcap);
   unsigned char* base = qsm + (threadIdx.x >> 5) * per;
   WarpScratch<T, D> ws;
   ws.buf = (PointRec<T, D>*)base;
   base += stage_bytes<T, D>();
   ws.stack = (int*)base;
   base += ((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15;
-  ws.dmat = nullptr;
-  ws.cid = nullptr;
-  ws.rows = nullptr;
-  ws.kst = nullptr;
-  ws.excl = nullptr;
-  if (coop) {
-    ws.rows = (unsigned long long*)base;
-    base += (size_t)32 * (coop + 1) * 8;
-    ws.kst = (unsigned long long*)base;
-    base += (size_t)(32 / coop) * 32 * 8;
-    ws.excl = (int4*)base;
-    base += 32 * 16;
-  } else {
-    ws.dmat = (DistT*)base;
-    base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
-    ws.cid = (int*)base;
-    base += 32 * 4;
-  }
+  ws.dmat = (DistT*)base;
+  base += (32 * 33 * sizeof(DistT) + 15) & ~(size_t)15;
+  ws.cid = (int*)base;
+  base += 32 * 4;
   ws.log = logcap ? (int*)base : nullptr;
   return ws;
-}
-
-// The list capacity whose packet walks use cooperative shared-memory lists
-// (packet_knn_coop), or 0: float distances and capacities up to 32.
-template <typename T, int KMAX>
-__host__ __device__ constexpr int coop_kmax() {
-  return (std::is_same<typename DistOf<T>::type, float>::value && KMAX <= 32) ? KMAX : 0;
 }
 
 // Candidate-log capacity per lane of the normals kernel.
@@ -276,13 +248,14 @@ __device__ __forceinline__ float seed_bound32(const TreeView<T, D>& tv, const fl
 // candidates of the wider window outside [wlo, wlo + wn) are offered by the
 // walk as any other.
 //
-// Float lists with k equal to their capacity (k = 4, 8, 16) start from a
-// window of 2k positions instead: the list then holds the k nearest of 2k
-// tree-order neighbours, all of them real candidates.
+// Float lists with k equal to their capacity (k = 4, 8, 16, 32) start from
+// a window of warm_mult x k positions instead (g_tune_warm_mult >= 2): the
+// list then holds the k nearest of those tree-order neighbours, all of them
+// real candidates.
 template <typename T, int D, typename DistT, typename Top>
 __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, const SlotMap& fm, int slot,
                                           const DistT* q, int anchor, int k, int own, DistT r2, bool bound,
-                                          int& wlo, int& wn) {
+                                          int warm_mult, int& wlo, int& wn) {
   constexpr int CAP = Top::CAP;
   wlo = 0;
   wn = 0;
@@ -294,38 +267,40 @@ __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, co
     hi = (int)fm.valid_off[c + 1];
   }
   if (hi <= lo) return;
-  if constexpr (std::is_same<DistT, float>::value && CAP <= 16) {
-    if (k == CAP) {
-      // twice as wide a window: its first CAP keys fill the list, the
-      // others are sorted apart and merged in, so the list holds the CAP
-      // nearest of 2 CAP tree-order neighbours (all real unless the window
-      // is short) and its bound is their CAP-th distance
-      constexpr int W = 2 * CAP;
+  if constexpr (std::is_same<DistT, float>::value && CAP <= 32) {
+    if (k == CAP && warm_mult >= 2) {
+      // a window of warm_mult x k positions: its first k keys fill the
+      // list, the rest are sorted apart in blocks of Q and merged in, so the
+      // list holds the k nearest of the window's tree-order neighbours (all
+      // real unless the window is short) and its bound is their k-th distance
+      constexpr int Q = CAP < 16 ? CAP : 16;
+      const int W = warm_mult * CAP;
       const int a2 = min(max(anchor, lo), hi - 1);
-      const int start = hi - lo >= W ? min(max(a2 - CAP, lo), hi - W) : lo;
-      unsigned long long t[CAP];
-#pragma unroll
-      for (int j = 0; j < W; j++) {
-        const int p = start + j;
+      const int start = hi - lo >= W ? min(max(a2 - W / 2, lo), hi - W) : lo;
+      auto key_at = [&](int p) {
         unsigned long long key = top.key_empty();
         if (p < hi && p != own) {
           const PointRec<T, D> r = tv.pts[p];
           const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
           if (d2 < r2) key = top.key_real(d2, r.id);
         }
-        if (j < CAP)
-          top.s[j] = key;
-        else
-          t[j - CAP] = key;
-      }
+        return key;
+      };
+#pragma unroll
+      for (int j = 0; j < CAP; j++) top.s[j] = key_at(start + j);
       top.sort_desc();
-      bitonic_sort<CAP>(t, false);
-      top.merge_smallest(t);
+      for (int off = CAP; off < W; off += Q) {
+        unsigned long long t[Q];
+#pragma unroll
+        for (int j = 0; j < Q; j++) t[j] = key_at(start + off + j);
+        bitonic_sort<Q>(t, false);
+        top.merge_smallest(t);
+      }
       wlo = start;
       wn = min(W, hi - start);
-      // with CAP = 16 the window is seed_bound32's own: its bound is the
-      // list's already
-      if (bound && CAP < 16) top.seed(k, seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi), r2);
+      // a window narrower than seed_bound32's 32 positions: its bound may
+      // be tighter
+      if (bound && k <= 16 && W < 32) top.seed(k, seed_bound32<T, D>(tv, q, anchor, k, own, lo, hi), r2);
       return;
     }
   }
@@ -503,12 +478,11 @@ template <typename T, int D, int KMAX, typename L>
 __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename DistOf<T>::type))) k_knn(TreeView<T, D> tv, L ld, const int* order, int order_mode, int m,
                                                   int k, typename DistOf<T>::type r2, int32_t* out_idx,
                                                   int32_t* out_cnt, int* status, SlotMap fm, int lane_span,
-                                                  bool warm_bound) {
+                                                  bool warm_bound, int warm_mult) {
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  constexpr int COOP = coop_kmax<T, KMAX>();
-  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth, 0, COOP);
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
   int qid = -1, own = -1, anchor = -1;
   DistT q[D];
   bool active = false;
@@ -525,16 +499,10 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
   int wlo = 0, wn = 0;
-  if (active) warm_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
-  bool ok;
-  if (use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)) {
-    ok = lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top, wlo, wn);
-  } else {
-    if constexpr (COOP > 0)
-      ok = packet_knn_coop<KMAX, T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
-    else
-      ok = packet_knn<T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
-  }
+  if (active) warm_topk<T, D, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, warm_mult, wlo, wn);
+  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
+                      ? lane_knn<LANE_STACK, T, D>(tv, q, own, active, r2, top, wlo, wn)
+                      : packet_knn<T, D>(tv, q, own, active, r2, top, ws, wlo, wn);
   if (!ok) atomicExch(status, 1);
   if (qid >= 0) {
     int c = 0;
@@ -554,13 +522,14 @@ template <typename T, int D, int KMAX, typename L>
 void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                 int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth, 0, coop_kmax<T, KMAX>());
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
   if (smem > 48 * 1024)
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
                                                                       d_idx, d_cnt, status, fm,
                                                                       g_tune_lane_span.load(),
-                                                                      g_tune_warm_bound.load() != 0);
+                                                                      g_tune_warm_bound.load() != 0,
+                                                                      g_tune_warm_mult.load());
   PPTKG_CHECK_LAUNCH();
 }
 
@@ -1114,13 +1083,12 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
                                                       int* fix, int* nfix, int* status, SlotMap fm, int lane_span,
-                                                      bool warm_bound) {
+                                                      bool warm_bound, int warm_mult) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
-  constexpr int COOP = coop_kmax<T, KMAX>();
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP, COOP);
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
   const int lane = threadIdx.x & 31;
   int qid = -1, own = -1, grp = 0, anchor = -1;
   DistT q[3];
@@ -1138,16 +1106,10 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   TopK<KMAX, DistT> top;
   top.reset(k, r2);
   int wlo = 0, wn = 0;
-  if (active) warm_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, wlo, wn);
-  bool ok;
-  if (use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)) {
-    ok = lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top, wlo, wn);
-  } else {
-    if constexpr (COOP > 0)
-      ok = packet_knn_coop<KMAX, T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
-    else
-      ok = packet_knn<T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
-  }
+  if (active) warm_topk<T, 3, DistT>(top, tv, fm, slot, q, anchor, k, own, r2, warm_bound, warm_mult, wlo, wn);
+  const bool ok = use_lane_walk<LANE_STACK>(anchor, active, lane_span, tv.depth)
+                      ? lane_knn<LANE_STACK, T, 3>(tv, q, own, active, r2, top, wlo, wn)
+                      : packet_knn<T, 3>(tv, q, own, active, r2, top, ws, wlo, wn);
   if (!ok) atomicExch(status, 1);
   if (qid < 0) return;
   if (!active) {
@@ -1365,13 +1327,13 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
                     cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX), coop_kmax<T, KMAX>());
+  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
       view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm,
-      g_tune_lane_span.load(), g_tune_warm_bound.load() != 0);
+      g_tune_lane_span.load(), g_tune_warm_bound.load() != 0, g_tune_warm_mult.load());
   PPTKG_CHECK_LAUNCH();
 }
 

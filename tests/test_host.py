@@ -49,7 +49,8 @@ def test_tuning_knobs_validate_and_round_trip():
     for name, default, good, bad in (("lane_span", 1024, (-1, 0, 64, 1 << 20), (-2,)),
                                      ("rnear_warp_queries", 262144, (0, 1, 1 << 30), (-1,)),
                                      ("warm_bound", 1, (0, 1), (-1, 2)),
-                                     ("topk_min", 0, (4, 8, 16, 32, 64, 0), (-1, 3, 65, 128))):
+                                     ("topk_min", 0, (4, 8, 16, 32, 64, 0), (-1, 3, 65, 128)),
+                                     ("warm_mult", 2, (1, 3, 8, 2), (0, 9, -1))):
         assert N.tune_get(name) == default
         try:
             for v in good:
