@@ -264,7 +264,6 @@ struct WarpScratch {
   int* log;                              // per-lane neighbour lists, lane-strided; null when unused
   typename DistOf<T>::type* dmat;        // 32 x 33 distances (kNN bucket scan); null when unused
   int* cid;                              // 32 candidate ids of the chunk being scanned (kNN)
-  unsigned long long* pend;              // deferred candidate keys, lane-strided; null when unused
 };
 
 // A lane's query as the rest of its warp reads it during a bucket scan:
@@ -434,48 +433,16 @@ __device__ __forceinline__ bool packet_walk(const TreeView<T, D>& tv, const Dist
   return ok;
 }
 
-// Capacity of the deferred-candidate buffer of a float list of capacity
-// KMAX (packet_knn), in keys per lane.
-__host__ __device__ constexpr int pend_cap(int kmax) { return kmax < 16 ? kmax : 16; }
-
 // Exact kNN of the lane's query over the whole tree, ties in dist2 broken by
 // point id, with the top-k list in the lane's registers.  `own` (tree
 // position or -1) is skipped, which is how self queries exclude the query
 // point itself; so are the tree positions [wlo, wlo + wn), the warm-start
 // window whose candidates the list holds.
-//
-// Float lists defer their insertions: the candidates a bucket scan marks for
-// a lane (those within the list's bound at the time) go to the lane's
-// buffer ws.pend, and when some lane's buffer is full, and at the end of the
-// walk, every lane merges its buffer into its list at once -- a bitonic sort
-// of the buffer and a bitonic merge, the same instructions on all 32 lanes.
-// Inserting each candidate as it comes runs a KMAX-wide compare network on
-// the lanes that have one while the others wait, once per candidate, and
-// the candidates of a bucket belong to a third of the lanes or fewer.  The
-// bound moves only at merges, so a few more candidates are marked and a
-// few more nodes visited; the result (the k smallest (dist2, id) pairs of
-// all candidates) is the same.
 template <typename T, int D, typename Top, typename DistT>
 __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool active, DistT r2, Top& top,
                            WarpScratch<T, D> ws, int wlo = 0, int wn = 0) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xffffffffu;
-  constexpr bool DEFER = std::is_same<DistT, float>::value;
-  constexpr int PCAP = pend_cap(Top::CAP);
-  int pcnt = 0;
-  // merges the lane's deferred candidates into its list (warp-uniform call)
-  auto flush = [&]() {
-    if constexpr (DEFER) {
-      if (!__any_sync(FULL, pcnt > 0)) return;
-      unsigned long long t[PCAP];
-#pragma unroll
-      for (int j = 0; j < PCAP; j++) t[j] = j < pcnt ? ws.pend[j * 32 + lane] : top.key_empty();
-      bitonic_sort<PCAP>(t, false);
-      top.merge_smallest(t);
-      pcnt = 0;
-      __syncwarp();
-    }
-  };
   auto need = [&](DistT md) { return active && md < r2 && md <= top.worst(); };
   // Leaf bucket scan, transposed: lane j holds candidate j of the chunk
   // (one coalesced 16 B load), and the warp loops only over the lanes whose
@@ -525,30 +492,16 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
       if (own >= base && own < base + nb) mark &= ~(1u << (own - base));
       mark &= ~window_bits(wlo - base, wn);
       __syncwarp();
-      if constexpr (DEFER) {
-        // append to the buffer, merging whenever a buffer is full
-        while (__any_sync(FULL, mark != 0u)) {
-          if (__any_sync(FULL, pcnt == PCAP)) flush();
-          if (mark) {
-            const int t = __ffs(mark) - 1;
-            mark &= mark - 1;
-            ws.pend[pcnt * 32 + lane] = top.key_real(ws.dmat[lane * 33 + t], ws.cid[t]);
-            pcnt++;
-          }
-        }
-      } else {
-        while (mark) {
-          const int t = __ffs(mark) - 1;
-          mark &= mark - 1;
-          top.offer(ws.dmat[lane * 33 + t], ws.cid[t]);
-        }
+      top.reserve(__popc(mark));
+      while (mark) {
+        const int t = __ffs(mark) - 1;
+        mark &= mark - 1;
+        top.offer(ws.dmat[lane * 33 + t], ws.cid[t]);
       }
       __syncwarp();
     }
   };
-  const bool ok = packet_walk<T, D, DistT>(tv, q, active, ws, need, scan);
-  flush();
-  return ok;
+  return packet_walk<T, D, DistT>(tv, q, active, ws, need, scan);
 }
 
 // Per-lane traversal for warps whose queries lie far apart, where a packet

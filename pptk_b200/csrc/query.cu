@@ -32,38 +32,26 @@ TreeView<T, D> view_of(const TreeBase* t) {
 
 // Per-warp shared memory: the staging buffer (a leaf chunk in r-near walks,
 // the warp's queries in kNN walks), traversal stack, the 32 x 33 distance
-// matrix and the 32 candidate ids of the kNN bucket scan, and one region
-// holding (normals, after the walk) `logcap` list slots per lane and
-// (float kNN walks, during it) `pendcap` deferred candidate keys per lane.
+// matrix and the 32 candidate ids of the kNN bucket scan, and (normals)
+// `logcap` list slots per lane.
 template <typename T, int D>
 __host__ __device__ constexpr size_t stage_bytes() {
   typedef typename DistOf<T>::type DistT;
   return 32 * (sizeof(PointRec<T, D>) > sizeof(QStage<DistT, D>) ? sizeof(PointRec<T, D>) : sizeof(QStage<DistT, D>));
 }
 
-__host__ __device__ constexpr size_t tail_bytes(int logcap, int pendcap) {
-  return (size_t)logcap * 32 * 4 > (size_t)pendcap * 32 * 8 ? (size_t)logcap * 32 * 4 : (size_t)pendcap * 32 * 8;
-}
-
 template <typename T, int D>
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0, int pendcap = 0) {
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
   return stage_bytes<T, D>() + (((size_t)depth * sizeof(StackEnt<T, D>) + 15) & ~(size_t)15) +
-         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4 + tail_bytes(logcap, pendcap);
-}
-
-// Deferred-candidate buffer capacity of the kNN / normals kernels with list
-// capacity KMAX: float lists only (packet_knn).
-template <typename T, int KMAX>
-__host__ __device__ constexpr int pend_cap_of() {
-  return std::is_same<typename DistOf<T>::type, float>::value ? pend_cap(KMAX) : 0;
+         ((32 * 33 * sizeof(DistT) + 15) & ~(size_t)15) + 32 * 4 + (size_t)logcap * 32 * 4;
 }
 
 template <typename T, int D>
-__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0, int pendcap = 0) {
+__device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap = 0) {
   typedef typename DistOf<T>::type DistT;
   extern __shared__ __align__(16) unsigned char qsm[];
-  const size_t per = warp_smem_bytes<T, D>(depth, logcap, pendcap);
+  const size_t per = warp_smem_bytes<T, D>(depth, logcap);
   unsigned char* base = qsm + (threadIdx.x >> 5) * per;
   WarpScratch<T, D> ws;
   ws.buf = (PointRec<T, D>*)base;
@@ -75,7 +63,6 @@ __device__ __forceinline__ WarpScratch<T, D> warp_scratch(int depth, int logcap 
   ws.cid = (int*)base;
   base += 32 * 4;
   ws.log = logcap ? (int*)base : nullptr;
-  ws.pend = pendcap ? (unsigned long long*)base : nullptr;
   return ws;
 }
 
@@ -495,7 +482,7 @@ __global__ void __launch_bounds__(QTHREADS, knn_min_blocks(KMAX, sizeof(typename
   typedef typename DistOf<T>::type DistT;
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth, 0, pend_cap_of<T, KMAX>());
+  WarpScratch<T, D> ws = warp_scratch<T, D>(tv.depth);
   int qid = -1, own = -1, anchor = -1;
   DistT q[D];
   bool active = false;
@@ -535,7 +522,7 @@ template <typename T, int D, int KMAX, typename L>
 void launch_knn(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                 int32_t* d_idx, int32_t* d_cnt, int* status, cudaStream_t st, SlotMap fm) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth, 0, pend_cap_of<T, KMAX>());
+  const size_t smem = QWARPS * warp_smem_bytes<T, D>(t->tdepth);
   if (smem > 48 * 1024)
     PPTKG_CUDA(cudaFuncSetAttribute(k_knn<T, D, KMAX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<T, D, KMAX, L><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(view_of<T, D>(t), ld, order, mode, m, k, r2,
@@ -1101,7 +1088,7 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
   if ((slot & ~31) >= m) return;
-  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP, pend_cap_of<T, KMAX>());
+  WarpScratch<T, 3> ws = warp_scratch<T, 3>(tv.depth, LOGCAP);
   const int lane = threadIdx.x & 31;
   int qid = -1, own = -1, grp = 0, anchor = -1;
   DistT q[3];
@@ -1340,7 +1327,7 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
                     cudaStream_t st, SlotMap fm = SlotMap{}) {
   if (m <= 0) return;
-  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX), pend_cap_of<T, KMAX>());
+  const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
   if (smem > 48 * 1024)
     PPTKG_CUDA(
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
