@@ -481,6 +481,21 @@ def run_ragged_workload(args, ctx):
     ms_q, _, _ = device_timed(ctx, lambda: (cap_k.replay(), cap_n.replay()), args.steps)
     cap_k.check()
     cap_n.check()
+    del cap_k, cap_n
+    # the whole step (forest rebuild from the points + kNN + normals)
+    # replayed from one CUDA graph; its results are checked against the
+    # direct calls once
+    buf = dev.clone()
+    l0 = ctx.lib.pptkg_launch_count()
+    cap_p, outs = f.capture_pipeline(buf, k)
+    kernels_p = (ctx.lib.pptkg_launch_count() - l0) // 2  # one direct pass, one captured
+    ms_p, _, _ = device_timed(ctx, cap_p.replay, args.steps)
+    cap_p.check()
+    ref_i, ref_c = f.knn(k)
+    pipeline_ok = bool(torch.equal(outs["indices"], ref_i) and torch.equal(outs["counts"], ref_c)
+                       and torch.equal(torch.nan_to_num(outs["normals"], nan=-9.0),
+                                       torch.nan_to_num(f.normals(k), nan=-9.0)))
+    del cap_p, outs, ref_i, ref_c
     e2e = None
     if not args.no_e2e:
         host = torch.from_numpy(P).pin_memory().numpy()
@@ -507,6 +522,11 @@ def run_ragged_workload(args, ctx):
             "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
                              "ms_per_step": ms_q, "what": "kNN + normals of every point, replayed from two CUDA "
                                                          "graphs on the built forest"},
+            "graph_pipeline": {"value": ctx.world * n / (ctx.max_over_ranks(ms_p) / 1e3), "unit": "points/s",
+                               "ms_per_step": ms_p, "direct_ms_per_step": ms_max, "equal_to_direct": pipeline_ok,
+                               "kernels_in_graph": kernels_p,
+                               "what": "the whole step (forest rebuild + kNN + normals) replayed from one CUDA "
+                                       "graph on a capture-ready forest"},
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof,
             "cpu_baseline": None, "clocks": clk}
 
@@ -1010,6 +1030,9 @@ def run_config(name, args, ctx):
         summary["stage_ms"] = {k: round(v["ms_per_step"], 1) for k, v in st.items()
                                if k in ("build", "forest.knn", "forest.normals")}
         summary["graph_replay_queries_ms"] = round(res["graph_replay"]["ms_per_step"], 1)
+        gp = res["graph_pipeline"]
+        summary["graph_step_ms"] = round(gp["ms_per_step"], 1)
+        summary["graph_step_equal"] = gp["equal_to_direct"]
         summary["e2e_value"] = (res["e2e"] or {}).get("value")
     elif name == "multitree":
         lq, lh = _lat(res["latency"]), _lat(res["latency_at_half_load"])

@@ -210,6 +210,26 @@ PPTKG_API int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int
 PPTKG_API int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
                                    void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream);
 
+/* Capture mode of a float32 / float64 forest (no reference counterpart; the
+ * rebuild step of a CUDA graph over build and queries).
+ * pptkg_forest_capture_ready sizes the forest's device arrays for new
+ * coordinates of the same rows and fixes the rebuild's launch shapes, then
+ * synchronises.  After it,
+ * pptkg_forest_rebuild rebuilds every cloud's tree in place from new
+ * coordinates of the same n rows (points: device, the layout of
+ * pptkg_forest_build) with no host synchronisation while a status sink is
+ * set, so that rebuild, pptkg_forest_knn and pptkg_forest_normals can be
+ * captured together; the trees equal those pptkg_forest_build gives for the
+ * new coordinates.  The capacities are the first build's tree levels + 8
+ * and twice its records and traversal nodes; sink code 20 (more levels) or
+ * 21 (more records), without a sink PPTKG_E_UNSUPPORTED, means the
+ * coordinates need more than that: the trees of that pass are not the
+ * reference trees and the forest must be built again.  Host-side reads
+ * (pptkg_forest_info, pptkg_tree_info, ref nodes, save) synchronise the
+ * device and take the last rebuild's counts. */
+PPTKG_API int pptkg_forest_capture_ready(pptkg_tree* forest, void* stream);
+PPTKG_API int pptkg_forest_rebuild(pptkg_tree* forest, const void* points, void* stream);
+
 /* Multi-tree batches (no reference counterpart; the serving loop's batching
  * step).  One launch answers queries for several resident single trees:
  * tree g answers the concatenated query rows [row_offsets[g],

@@ -158,7 +158,8 @@ void dispatch_query_dims(const TreeBase* t, F&& f) {
   });
 }
 
-const TreeBase* tree_of(const pptkg_tree* t) {
+// The tree of a handle, for the capturable forest entries (no host work).
+TreeBase* tree_raw(const pptkg_tree* t) {
   if (!t || !t->t) throw Error(E_INVALID, "null tree");
   return t->t.get();
 }
@@ -174,6 +175,27 @@ struct DeviceGuard {
     if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
   }
 };
+
+// The tree of a handle with host-side counts that match the device: a
+// capture-ready forest's last rebuild is read back first (a device-wide
+// synchronisation; these entries are not captured).
+const TreeBase* tree_of(const pptkg_tree* h) {
+  TreeBase* t = tree_raw(h);
+  if (t->capture) {
+    DeviceGuard g(t->device);
+    PPTKG_CUDA(cudaDeviceSynchronize());
+    dispatch_float(t->dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      switch (t->dim) {
+        case 2: forest_sync<T, 2>(t, 0); break;
+        case 3: forest_sync<T, 3>(t, 0); break;
+        default: forest_sync<T, 4>(t, 0); break;
+      }
+    });
+  }
+  return t;
+}
+
 
 constexpr int DEFAULT_BUCKET = 64;
 constexpr double DEFAULT_GAP = 1e-3;
@@ -319,6 +341,54 @@ int pptkg_forest_build(const void* points, int64_t n, int dim, int dtype, int me
   });
 }
 
+int pptkg_forest_capture_ready(pptkg_tree* forest, void* stream) {
+  return guarded([&] {
+    TreeBase* t = const_cast<TreeBase*>(tree_of(forest));
+    DeviceGuard g(t->device);
+    if (t->rec_dtype != F32 && t->rec_dtype != F64)
+      throw Error(E_TYPE, "capture mode needs a float32 or float64 forest");
+    dispatch_build(t->dtype, t->dim, [&](auto tt, auto d) {
+      typedef decltype(tt) T;
+      constexpr int Dm = decltype(d)::value;
+      forest_capture_ready<T, Dm>(t, S(stream));
+    });
+    forest_slot_map_device(t, S(stream));
+    PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+  });
+}
+
+int pptkg_forest_rebuild(pptkg_tree* forest, const void* points, void* stream) {
+  return guarded([&] {
+    TreeBase* t = tree_raw(forest);
+    DeviceGuard g(t->device);
+    if (!t->capture) throw Error(E_INVALID, "pptkg_forest_rebuild needs a capture-ready forest");
+    if (t->n > 0 && !points) throw Error(E_INVALID, "points is null");
+    // with a status sink set nothing is read back (the call can be
+    // captured); otherwise the status is checked here
+    DevBuf<int> own;
+    int* status = g_status_sink;
+    if (!status) {
+      own.alloc(1, S(stream));
+      PPTKG_CUDA(cudaMemsetAsync(own.get(), 0, sizeof(int), S(stream)));
+      status = own.get();
+    }
+    dispatch_build(t->dtype, t->dim, [&](auto tt, auto d) {
+      typedef decltype(tt) T;
+      constexpr int Dm = decltype(d)::value;
+      rebuild_forest<T, Dm>(t, (const T*)points, S(stream), status);
+    });
+    forest_slot_map_device(t, S(stream));
+    if (!g_status_sink) {
+      int h = 0;
+      PPTKG_CUDA(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+      PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+      if (h == 20) throw Error(E_UNSUPPORTED, "forest rebuild: the points need more tree levels than planned");
+      if (h == 21) throw Error(E_UNSUPPORTED, "forest rebuild: the points need more tree records than planned");
+      if (h) throw Error(E_DEVICE, "forest rebuild: device check failed (code " + std::to_string(h) + ")");
+    }
+  });
+}
+
 int pptkg_forest_info(const pptkg_tree* forest, int* ncloud, int64_t* valid_offsets) {
   return guarded([&] {
     const TreeBase* t = tree_of(forest);
@@ -339,7 +409,7 @@ int pptkg_forest_ref_nodes(const pptkg_tree* forest, int cloud, double* out, int
 int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int exclude_self, int mem, int32_t* out_idx,
                      int32_t* out_cnt, void* stream) {
   return guarded([&] {
-    const TreeBase* t = tree_of(forest);
+    const TreeBase* t = tree_raw(forest);
     DeviceGuard g(t->device);
     if (k < 1) throw Error(E_INVALID, "k must be positive");
     if (!(dmax >= 0.0)) throw Error(E_INVALID, "dmax must be non-negative");
@@ -360,7 +430,7 @@ int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int exclude_s
 int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
                          void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream) {
   return guarded([&] {
-    const TreeBase* t = tree_of(forest);
+    const TreeBase* t = tree_raw(forest);
     DeviceGuard g(t->device);
     if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
     if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
@@ -518,8 +588,8 @@ int pptkg_tree_ref_nodes(const pptkg_tree* tree, double* out, int64_t capacity, 
 
 int pptkg_tree_set_bucket(pptkg_tree* tree, int bucket, void* stream) {
   return guarded([&] {
-    if (!tree || !tree->t) throw Error(E_INVALID, "null tree");
-    TreeBase* t = tree->t.get();
+    // (a capture-ready forest's counts are synchronised first)
+    TreeBase* t = const_cast<TreeBase*>(tree_of(tree));
     DeviceGuard g(t->device);
     if (bucket < 1 || bucket > 4096) throw Error(E_INVALID, "bucket must be in [1, 4096]");
     dispatch_build_any(t->rec_dtype, t->dim, [&](auto tt, auto d) {

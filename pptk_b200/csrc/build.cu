@@ -803,8 +803,9 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
 
 // ------------------------------------------------------- finishing ----
 template <typename T, int D>
-__global__ void k_finish(SoA<T, D> soa, int nv, PointRec<T, D>* pts, int* fwd) {
+__global__ void k_finish(SoA<T, D> soa, int nv, PointRec<T, D>* pts, int* fwd, const int64_t* nv_dev = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nv_dev) nv = (int)*nv_dev;  // capture mode: the valid count is on the device
   if (i >= nv) return;
   PointRec<T, D> r;
 #pragma unroll
@@ -815,17 +816,28 @@ __global__ void k_finish(SoA<T, D> soa, int nv, PointRec<T, D>* pts, int* fwd) {
 }
 
 template <typename T, int D>
-__global__ void k_tflag(const Rec<T, D>* recs, int n_recs, int bucket, int* flag) {
+__global__ void k_tflag(const Rec<T, D>* recs, int n_recs, int bucket, int* flag, const int* n_dev = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_recs) return;
+  if (n_dev && i >= *n_dev) {  // capture mode: records beyond the live count
+    flag[i] = 0;
+    return;
+  }
   const Rec<T, D>& r = recs[i];
   flag[i] = (r.split_dim >= 0 && r.end - r.begin > bucket && r.left >= 0 && r.right >= 0) ? 1 : 0;
 }
 
 template <typename T, int D>
-__global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, const int* tid, TNode<T, D>* nodes) {
+__global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, const int* tid, TNode<T, D>* nodes,
+                        const int* n_dev = nullptr, int node_lim = INT_MAX, int* status = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_recs || !flag[i]) return;
+  if (i >= n_recs || (n_dev && i >= *n_dev) || !flag[i]) return;
+  // capture mode: nodes beyond the capacity are left out (their parents
+  // see them as buckets: the walks stay exact) and reported
+  if (tid[i] >= node_lim) {
+    atomicExch(status, 21);
+    return;
+  }
   const Rec<T, D>& r = recs[i];
   TNode<T, D> t;
   for (int c = 0; c < 2; c++) {
@@ -836,7 +848,7 @@ __global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, cons
       t.hi[c][d] = cr.hi[d];
     }
     t.cnt[c] = cr.end - cr.begin;
-    t.ref[c] = flag[ch] ? tid[ch] : -cr.begin - 1;
+    t.ref[c] = (flag[ch] && tid[ch] < node_lim) ? tid[ch] : -cr.begin - 1;
   }
   nodes[tid[i]] = t;
 }
@@ -846,9 +858,11 @@ __global__ void k_tfill(const Rec<T, D>* recs, int n_recs, const int* flag, cons
 // whole cloud as one bucket (or nothing, for a cloud without valid points).
 template <typename T, int D>
 __global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64_t* valid_off, int ncloud,
-                         const int* flag, const int* tid, int nt, TNode<T, D>* nodes, int* root_tnode) {
+                         const int* flag, const int* tid, int nt, TNode<T, D>* nodes, int* root_tnode,
+                         const int* nt_dev = nullptr) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncloud) return;
+  if (nt_dev) nt = *nt_dev;  // the node count on the device
   const int r = root_rec[c];
   TNode<T, D> t;
   for (int k = 0; k < 2; k++)
@@ -858,7 +872,7 @@ __global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64
     }
   t.ref[0] = t.ref[1] = -1;
   t.cnt[0] = t.cnt[1] = 0;
-  if (r >= 0 && flag[r]) {
+  if (r >= 0 && flag[r] && tid[r] < nt) {
     // the root record has its own node; the reserved slot stays an empty
     // node (nothing refers to it, but every slot holds a well-formed node)
     nodes[nt + c] = t;
@@ -1115,6 +1129,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
         throw Error(E_DEVICE, "device build: subtree check failed (code " + std::to_string(hctl.status) + ")");
     }
     tree->n_recs = hctl.rec_count;
+    tree->levels = levels;
     depth = std::max(depth, hctl.depth);
     break;
   }
@@ -1189,9 +1204,13 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
     PPTKG_CUDA(cudaStreamSynchronize(st));
   }
   TNode<T, D>* nodes = nullptr;
-  PPTKG_CUDA(dev_malloc((void**)&nodes, (size_t)(nt + tree->ncloud) * sizeof(TNode<T, D>), st));
+  // a capture-ready forest keeps the capacity that its rebuilds fill
+  const int64_t cap = tree->capture ? std::max<int64_t>(tree->cap_tnodes, (int64_t)nt + tree->ncloud)
+                                    : (int64_t)nt + tree->ncloud;
+  if (tree->capture) tree->cap_tnodes = cap;
+  PPTKG_CUDA(dev_malloc((void**)&nodes, (size_t)cap * sizeof(TNode<T, D>), st));
   tree->tnodes = nodes;
-  tree->n_tnodes = nt + tree->ncloud;
+  tree->n_tnodes = (int)cap;
   if (nt > 0) {
     k_tfill<T, D><<<div_up(nr, 256), 256, 0, st>>>(recs, nr, flag.get(), tid.get(), nodes);
     PPTKG_CHECK_LAUNCH();
@@ -1203,10 +1222,219 @@ void make_tnodes(TreeBase* tree, int bucket, cudaStream_t st) {
   tree->root_tnode_h.resize(tree->ncloud);
   PPTKG_CUDA(cudaMemcpyAsync(tree->root_tnode_h.data(), tree->root_tnode, sizeof(int) * tree->ncloud,
                              cudaMemcpyDeviceToHost, st));
-  tree->tdepth = tree->depth + 2;
+  if (!tree->capture) tree->tdepth = tree->depth + 2;
   if constexpr (std::is_integral<T>::value) lower_tnodes<T, D>(tree, st);
   PPTKG_CUDA(cudaStreamSynchronize(st));
 }
+
+#ifndef PPTKG_BUILD_INT
+// ------------------------------------------------------ capture mode ----
+// Build status of a rebuild: the device checks of the build kernels, code
+// 20 when the new data needs a deeper tree than the capacity planned for
+// (large segments left after the last of the cap_levels levels, or a depth
+// beyond the traversal stacks' tdepth) and 21 when it needs more records.
+// meta: valid points, records, depth.
+static __global__ void k_rebuild_status(const BuildCtl* ctl, int levels_cap, int tdepth, int* status, int64_t* meta,
+                                        const int64_t* valid_off, int ncloud) {
+  int levels = 0;
+  for (int l = 0; l < levels_cap; l++)
+    if (ctl->level_cnt[l] > 0) levels = l + 1;
+  const int depth = ctl->depth > levels ? ctl->depth : levels;
+  if (ctl->status) atomicExch(status, ctl->status == 6 ? 21 : 10 + ctl->status);
+  if (ctl->level_cnt[levels_cap] > 0 || depth + 2 > tdepth) atomicExch(status, 20);
+  meta[0] = valid_off[ncloud];
+  meta[1] = ctl->rec_count;
+  meta[2] = depth;
+  meta[3] = 0;
+}
+
+template <typename T, int D>
+void forest_capture_ready(TreeBase* t, cudaStream_t st) {
+  if (t->capture) return;
+  if (t->rec_dtype != F32 && t->rec_dtype != F64) throw Error(E_TYPE, "capture mode needs float32 or float64 points");
+  int cap_list;
+  size_t smem;
+  const int small_cap = small_capacity<T, D>(t->max_leaf, cap_list, smem);
+  const int64_t n = t->n;
+  t->cap_levels = std::min(t->levels + 8, MAX_LEVELS);
+  const int64_t seg_cap = n / (small_cap + 1) + 2;
+  // small segments: at most two children of every large segment of every
+  // level, plus the clouds' roots
+  const int64_t small = 2 * (int64_t)t->cap_levels * (seg_cap + 1) + t->ncloud + 64;
+  if (small > INT32_MAX) throw Error(E_INVALID, "forest too large for capture mode");
+  t->cap_small = (int)small;
+  // records and traversal nodes: twice the first build's counts (a tree
+  // over n points has at most 2n - 1 records); a rebuild that needs more
+  // stops with code 21
+  t->cap_recs = std::min<int64_t>(2 * n + 64, 2 * (int64_t)t->n_recs + 4096);
+  // (the direct build's inner traversal nodes: n_tnodes less the clouds'
+  // root slots)
+  const int64_t live_tnodes = std::max<int64_t>((int64_t)t->n_tnodes - t->ncloud, 0);
+  t->cap_tnodes = std::min<int64_t>(t->cap_recs, 2 * live_tnodes + 4096) + t->ncloud;
+  if (t->cap_recs > INT32_MAX / 2 || t->cap_tnodes > INT32_MAX / 2)
+    throw Error(E_INVALID, "forest too large for capture mode");
+  int per_sm = 1, nsm = 1;
+  PPTKG_CUDA(cudaFuncSetAttribute(k_subtree<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PPTKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subtree<T, D>, SUB_THREADS, smem));
+  PPTKG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, t->device));
+  t->cap_subgrid = std::max(per_sm, 1) * nsm;
+  // capacity-sized arrays, current contents kept
+  auto grow = [&](void** p, size_t have, size_t want) {
+    void* q = nullptr;
+    PPTKG_CUDA(dev_malloc(&q, std::max<size_t>(want, 1), st));
+    if (have) PPTKG_CUDA(cudaMemcpyAsync(q, *p, have, cudaMemcpyDeviceToDevice, st));
+    if (*p) dev_free(*p, st);
+    *p = q;
+  };
+  grow(&t->pts, (size_t)t->nv * sizeof(PointRec<T, D>), (size_t)n * sizeof(PointRec<T, D>));
+  grow(&t->recs, (size_t)t->n_recs * sizeof(Rec<T, D>), (size_t)t->cap_recs * sizeof(Rec<T, D>));
+  grow(&t->tnodes, (size_t)t->n_tnodes * sizeof(TNode<T, D>), (size_t)t->cap_tnodes * sizeof(TNode<T, D>));
+  t->n_tnodes = (int)t->cap_tnodes;
+  t->tdepth += 8;
+  if (!t->dev_meta) PPTKG_CUDA(dev_malloc((void**)&t->dev_meta, 4 * sizeof(int64_t), st));
+  t->capture = true;
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename T, int D>
+void rebuild_forest(TreeBase* t, const T* d_in, cudaStream_t st, int* status) {
+  if (!t->capture) throw Error(E_INVALID, "rebuild needs a capture-ready forest");
+  Stage stage("rebuild", st);
+  const int64_t n = t->n;
+  const int ncloud = t->ncloud;
+  // valid rows and per-cloud valid offsets, all on the device
+  BuildBuf<int> flag(n + 1, st), off(n + 1, st);
+  if (n > 0) {
+    k_valid<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get());
+    PPTKG_CHECK_LAUNCH();
+  }
+  exclusive_scan<int, int>(flag.get(), off.get(), n, off.get() + n, st);
+  k_cloud_off<<<div_up(ncloud + 1, 256), 256, 0, st>>>(off.get(), t->orig_off, ncloud, t->valid_off);
+  PPTKG_CHECK_LAUNCH();
+  BuildBuf<T> xs((size_t)D * n + 1, st);
+  BuildBuf<int> ids(n + 1, st);
+  SoA<T, D> soa;
+  for (int d = 0; d < D; d++) soa.x[d] = xs.get() + (size_t)d * n;
+  soa.id = ids.get();
+  if (n > 0) {
+    k_compact<T, D><<<div_up(n, 256), 256, 0, st>>>(d_in, n, flag.get(), off.get(), soa);
+    PPTKG_CHECK_LAUNCH();
+  }
+  flag.release();
+  off.release();
+  int cap_list;
+  size_t smem;
+  const int small_cap = small_capacity<T, D>(t->max_leaf, cap_list, smem);
+  const int rec_cap = (int)t->cap_recs;
+  Rec<T, D>* recs = (Rec<T, D>*)t->recs;
+  const int seg_cap = (int)(n / (small_cap + 1) + 2);
+  const int max_tiles = (int)(n / TILE) + seg_cap + 2;
+  BuildBuf<BuildCtl> ctl(1, st);
+  PPTKG_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(BuildCtl), st));
+  PPTKG_CUDA(cudaMemsetAsync(t->root_rec, 0xff, sizeof(int) * ncloud, st));
+  BuildBuf<Seg<T, D>> segL[2] = {BuildBuf<Seg<T, D>>(seg_cap, st), BuildBuf<Seg<T, D>>(seg_cap, st)};
+  BuildBuf<Seg<T, D>> smallL(t->cap_small, st);
+  k_roots<T, D><<<div_up(ncloud, 128), 128, 0, st>>>(t->valid_off, t->orig_off, ncloud, small_cap, segL[0].get(),
+                                                      smallL.get(), t->cap_small, ctl.get());
+  PPTKG_CHECK_LAUNCH();
+  {
+    // a fixed number of levels; the kernels of a level without segments
+    // return at once
+    BuildBuf<int> blpos(n + 1, st), grpos(n + 1, st);
+    BuildBuf<int> tile_seg(max_tiles, st);
+    BuildBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
+    const unsigned gt = (unsigned)max_tiles;
+    const unsigned gs = (unsigned)div_up(seg_cap, 128);
+    for (int lvl = 0; lvl < t->cap_levels; lvl++) {
+      Seg<T, D>* A = segL[lvl & 1].get();
+      Seg<T, D>* B = segL[(lvl + 1) & 1].get();
+      k_tiles<T, D><<<1, 1024, 0, st>>>(A, lvl, tile_seg.get(), ctl.get());
+      PPTKG_CHECK_LAUNCH();
+      k_seg_init<T, D><<<gs, 128, 0, st>>>(A, lvl, ctl.get());
+      PPTKG_CHECK_LAUNCH();
+      k_bbox<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa);
+      PPTKG_CHECK_LAUNCH();
+      k_node<T, D><<<gs, 128, 0, st>>>(A, lvl, ctl.get(), recs, rec_cap, t->root_rec, t->max_leaf, t->empty_split);
+      PPTKG_CHECK_LAUNCH();
+      k_count<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa);
+      PPTKG_CHECK_LAUNCH();
+      for (int pass = 1; pass <= 2; pass++) {
+        k_flags<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_cnt.get());
+        PPTKG_CHECK_LAUNCH();
+        k_tscan<T, D><<<(unsigned)seg_cap, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
+        PPTKG_CHECK_LAUNCH();
+        k_scatter<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_off.get(), blpos.get(),
+                                          grpos.get());
+        PPTKG_CHECK_LAUNCH();
+        k_swap<T, D><<<gt, BT, 0, st>>>(A, tile_seg.get(), ctl.get(), soa, blpos.get(), grpos.get());
+        PPTKG_CHECK_LAUNCH();
+      }
+      k_children<T, D><<<gs, 128, 0, st>>>(A, lvl, recs, B, smallL.get(), t->cap_small, small_cap, ctl.get());
+      PPTKG_CHECK_LAUNCH();
+    }
+  }
+  // the persistent subtree kernel takes the small segments; blocks without
+  // work return
+  k_subtree<T, D><<<t->cap_subgrid, SUB_THREADS, smem, st>>>(smallL.get(), soa, recs, t->root_rec, small_cap, cap_list,
+                                                             t->max_leaf, t->empty_split, rec_cap, ctl.get());
+  PPTKG_CHECK_LAUNCH();
+  k_rebuild_status<<<1, 1, 0, st>>>(ctl.get(), t->cap_levels, t->tdepth, status, t->dev_meta, t->valid_off, ncloud);
+  PPTKG_CHECK_LAUNCH();
+  // tree-ordered points and the forward map
+  if (n > 0) {
+    PPTKG_CUDA(cudaMemsetAsync(t->fwd, 0xff, n * sizeof(int), st));
+    k_finish<T, D><<<div_up(n, 256), 256, 0, st>>>(soa, (int)n, (PointRec<T, D>*)t->pts, t->fwd,
+                                                   t->valid_off + ncloud);
+    PPTKG_CHECK_LAUNCH();
+  }
+  // traversal hierarchy over the live records
+  BuildBuf<int> tflag(rec_cap + 1, st), tid(rec_cap + 1, st);
+  const int* nrec_dev = &ctl.get()->rec_count;
+  k_tflag<T, D><<<div_up(rec_cap, 256), 256, 0, st>>>(recs, rec_cap, t->bucket, tflag.get(), nrec_dev);
+  PPTKG_CHECK_LAUNCH();
+  exclusive_scan<int, int>(tflag.get(), tid.get(), rec_cap, tid.get() + rec_cap, st);
+  TNode<T, D>* nodes = (TNode<T, D>*)t->tnodes;
+  // inner nodes take the slots below cap_tnodes - ncloud, the clouds' root
+  // slots the last ncloud
+  const int node_lim = (int)(t->cap_tnodes - ncloud);
+  k_tfill<T, D><<<div_up(rec_cap, 256), 256, 0, st>>>(recs, rec_cap, tflag.get(), tid.get(), nodes, nrec_dev,
+                                                      node_lim, status);
+  PPTKG_CHECK_LAUNCH();
+  k_troots<T, D><<<div_up(ncloud, 128), 128, 0, st>>>(recs, t->root_rec, t->valid_off, ncloud, tflag.get(),
+                                                      tid.get(), node_lim, nodes, t->root_tnode);
+  PPTKG_CHECK_LAUNCH();
+}
+
+template <typename T, int D>
+void forest_sync(TreeBase* t, cudaStream_t st) {
+  if (!t->capture) return;
+  int64_t meta[4] = {0, 0, 0, 0};
+  PPTKG_CUDA(cudaMemcpyAsync(meta, t->dev_meta, sizeof(meta), cudaMemcpyDeviceToHost, st));
+  t->valid_off_h.resize(t->ncloud + 1);
+  PPTKG_CUDA(cudaMemcpyAsync(t->valid_off_h.data(), t->valid_off, sizeof(int64_t) * (t->ncloud + 1),
+                             cudaMemcpyDeviceToHost, st));
+  t->root_tnode_h.resize(t->ncloud);
+  PPTKG_CUDA(cudaMemcpyAsync(t->root_tnode_h.data(), t->root_tnode, sizeof(int) * t->ncloud, cudaMemcpyDeviceToHost,
+                             st));
+  int root0 = -1;
+  PPTKG_CUDA(cudaMemcpyAsync(&root0, t->root_rec, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PPTKG_CUDA(cudaStreamSynchronize(st));
+  if (meta[1] > 0) {  // a rebuild ran
+    t->nv = meta[0];
+    t->n_recs = (int)std::min<int64_t>(meta[1], t->cap_recs);  // (a rebuild past the capacity stops there)
+    t->depth = (int)meta[2];
+  }
+  if (root0 >= 0 && root0 < t->n_recs) {  // the first cloud's root box (saved with the tree)
+    Rec<T, D> r0;
+    PPTKG_CUDA(cudaMemcpyAsync(&r0, (const Rec<T, D>*)t->recs + root0, sizeof(r0), cudaMemcpyDeviceToHost, st));
+    PPTKG_CUDA(cudaStreamSynchronize(st));
+    for (int d = 0; d < D; d++) {
+      t->root_lo[d] = (double)r0.lo[d];
+      t->root_hi[d] = (double)r0.hi[d];
+    }
+  }
+}
+#endif  // PPTKG_BUILD_INT
 
 #ifndef PPTKG_BUILD_INT
 size_t TreeBase::device_bytes() const {
@@ -1227,6 +1455,7 @@ TreeBase::~TreeBase() {
   if (orig_off) dev_free(orig_off, stream);
   if (slot_off) dev_free(slot_off, stream);
   if (warp_cloud) dev_free(warp_cloud, stream);
+  if (dev_meta) dev_free(dev_meta, stream);
 }
 
 #endif  // PPTKG_BUILD_INT
@@ -1236,9 +1465,20 @@ TreeBase::~TreeBase() {
   template TreeBase* build_forest<T, D>(const T*, int64_t, const int64_t*, int, int, double, int, cudaStream_t); \
   template void make_tnodes<T, D>(TreeBase*, int, cudaStream_t);
 
+#define PPTKG_INST_CAPTURE(T, D)                                              \
+  template void forest_capture_ready<T, D>(TreeBase*, cudaStream_t);          \
+  template void rebuild_forest<T, D>(TreeBase*, const T*, cudaStream_t, int*); \
+  template void forest_sync<T, D>(TreeBase*, cudaStream_t);
+
 // This file builds float32 / float64 trees; build_int.cu includes it with
 // PPTKG_BUILD_INT set and builds the eight integer point types.
 #ifndef PPTKG_BUILD_INT
+PPTKG_INST_CAPTURE(float, 3)
+PPTKG_INST_CAPTURE(double, 3)
+PPTKG_INST_CAPTURE(float, 2)
+PPTKG_INST_CAPTURE(double, 2)
+PPTKG_INST_CAPTURE(float, 4)
+PPTKG_INST_CAPTURE(double, 4)
 PPTKG_INST_BUILD(float, 3)
 PPTKG_INST_BUILD(double, 3)
 PPTKG_INST_BUILD(float, 2)

@@ -1576,6 +1576,37 @@ static SlotMap slot_map(const TreeBase* t, int64_t& n_slots, cudaStream_t st) {
   return SlotMap{mt->warp_cloud, mt->slot_off, t->valid_off, t->root_tnode, nullptr, nullptr, nullptr};
 }
 
+#ifndef PPTKG_QUERY_DIM
+// Slots of each cloud rounded up to whole warps (capture mode: from the
+// device's valid offsets).
+static __global__ void k_slot_counts(const int64_t* valid_off, int ncloud, int64_t* cnt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncloud) cnt[c] = (valid_off[c + 1] - valid_off[c] + 31) / 32 * 32;
+}
+
+// The slot map of a capture-ready forest, computed on the device from its
+// current valid offsets over a fixed slot capacity (every cloud's input rows
+// rounded up to whole warps); warps beyond the live slots find no query.
+void forest_slot_map_device(TreeBase* t, cudaStream_t st) {
+  int64_t cap = 0;
+  for (int c = 0; c < t->ncloud; c++) cap += (t->orig_off_h[c + 1] - t->orig_off_h[c] + 31) / 32 * 32;
+  if (cap > INT32_MAX) throw Error(E_INVALID, "forest too large for one query pass");
+  const int64_t nw = std::max<int64_t>(cap / 32, 1);
+  if (!t->slot_off) PPTKG_CUDA(dev_malloc((void**)&t->slot_off, sizeof(int64_t) * (t->ncloud + 1), st));
+  if (!t->warp_cloud || t->n_slots != cap) {
+    if (t->warp_cloud) dev_free(t->warp_cloud, st);
+    PPTKG_CUDA(dev_malloc((void**)&t->warp_cloud, sizeof(int) * nw, st));
+  }
+  t->n_slots = cap;
+  DevBuf<int64_t> cnt(t->ncloud, st);
+  k_slot_counts<<<div_up(t->ncloud, 256), 256, 0, st>>>(t->valid_off, t->ncloud, cnt.get());
+  PPTKG_CHECK_LAUNCH();
+  exclusive_scan<int64_t, int64_t>(cnt.get(), t->slot_off, t->ncloud, t->slot_off + t->ncloud, st);
+  k_warp_cloud<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(t->slot_off, t->ncloud, nw, t->warp_cloud);
+  PPTKG_CHECK_LAUNCH();
+}
+#endif  // PPTKG_QUERY_DIM
+
 template <typename T, int D>
 void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_t* d_idx, int32_t* d_cnt,
                 cudaStream_t st) {
@@ -1615,7 +1646,9 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
   if (k > KNN_MAX_K) throw Error(E_UNSUPPORTED, "k > 64 is not supported by the GPU normal kernels");
   int64_t n_slots = 0;
   const SlotMap fm = slot_map(t, n_slots, st);
-  if (t->n > t->nv && t->n > 0) {
+  // rows of dropped points get NaN and size 0 (a capture-ready forest
+  // cannot tell from the host whether it has such rows)
+  if ((t->capture || t->n > t->nv) && t->n > 0) {
     k_fill_invalid<T><<<(unsigned)((t->n + 255) / 256), 256, 0, st>>>(t->n, num_eigen, d_evecs, d_evals, d_sizes);
     PPTKG_CHECK_LAUNCH();
   }

@@ -50,6 +50,9 @@ template <typename T>
 void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
                     T* d_evals, int32_t* d_sizes, cudaStream_t st);
 
+// Device-side slot map of a capture-ready forest (after each rebuild).
+void forest_slot_map_device(TreeBase* t, cudaStream_t st);
+
 // One launch over several single trees: tree g answers the query rows
 // [rows[g], rows[g+1]) (host offsets) of a concatenated batch.
 template <typename T, int D>

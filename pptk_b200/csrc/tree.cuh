@@ -97,6 +97,18 @@ struct TreeBase {
   int32_t* warp_cloud = nullptr;   // device [n_slots / 32]
   std::vector<int64_t> valid_off_h, orig_off_h;
   double root_lo[4] = {0, 0, 0, 0}, root_hi[4] = {0, 0, 0, 0};
+  int levels = 0;  // grid-wide build levels of the last direct build
+  // Capture mode (forest_capture_ready): the arrays have their capacities
+  // (points n, records cap_recs, traversal nodes cap_tnodes, query slots
+  // n_slots) and rebuild_forest issues no host synchronisation and no
+  // allocation whose size depends on device data, so it can be captured
+  // into a CUDA graph.  The host-side counts (nv, valid_off_h, n_recs,
+  // depth) are those of the last direct build or forest_sync; dev_meta
+  // holds the device's {nv, n_recs, depth, 0} of the last rebuild.
+  bool capture = false;
+  int cap_levels = 0, cap_small = 0, cap_subgrid = 0;
+  int64_t cap_recs = 0, cap_tnodes = 0;
+  int64_t* dev_meta = nullptr;
   size_t device_bytes() const;
   ~TreeBase();
 };

@@ -165,11 +165,84 @@ class Forest:
             return ev
         return ev, ew, sz
 
+    # ------------------------------------------------------- rebuilds --
+    def capture_ready(self):
+        """Sizes the forest's device arrays for rebuilds from any coordinates
+        of the same rows (capture mode).  After it, rebuild() and the
+        pipeline of capture_pipeline() rebuild the trees in place, without
+        host synchronisation."""
+        if not self._torch:
+            raise ValueError("capture mode needs a forest built from CUDA tensors")
+        N.call("pptkg_forest_capture_ready", self._h, self._stream, where="Forest.capture_ready()")
+        self._capture_mode = True
+
+    def _check_points(self, points):
+        import torch
+        if not N.is_torch_cuda(points) or points.device != self.device:
+            raise TypeError("points must be a CUDA tensor on the forest's device")
+        want = torch.float32 if self.dtype == np.float32 else torch.float64
+        if points.dtype != want or tuple(points.shape) != (self.n, self.dim) or not points.is_contiguous():
+            raise ValueError(f"points must be a contiguous ({self.n}, {self.dim}) tensor of {self.dtype}")
+
+    def refresh(self):
+        """Reads the valid offsets of the last (re)build back (after captured
+        rebuilds; waits for the device)."""
+        vo = np.empty(self.ncloud + 1, np.int64)
+        nc = ctypes.c_int()
+        N.call("pptkg_forest_info", self._h, ctypes.byref(nc), N.ptr(vo))
+        self.valid_offsets = vo
+        self.n_valid = int(vo[-1])
+
+    def rebuild(self, points):
+        """Rebuilds every cloud's tree from new coordinates of the same rows
+        (a contiguous CUDA tensor shaped like the build's points); the trees
+        equal those Forest(points, offsets) builds.  Needs capture_ready()."""
+        if not getattr(self, "_capture_mode", False):
+            raise ValueError("rebuild needs capture_ready() first")
+        self._check_points(points)
+        N.call("pptkg_forest_rebuild", self._h, N.ptr(points), self._stream, where="Forest.rebuild()")
+        self.refresh()
+
+    def capture_pipeline(self, points, k, r=math.inf, knn=True, normals=True, dmax=math.inf, exclude_self=True,
+                         precision="auto"):
+        """(CapturedQuery, outputs): one CUDA graph that rebuilds the forest
+        from `points` (a fixed CUDA tensor the caller refills between
+        replays), then runs Forest.knn (k, dmax, exclude_self) and / or
+        Forest.normals (k, r) into fixed tensors.  outputs: {"indices",
+        "counts", "normals"} as requested.  Calls capture_ready() if needed.
+        A replay whose points need a deeper tree than the first build's + 8
+        levels makes check() raise (build a new forest then)."""
+        from .estimate_normals import PRECISIONS
+        if not getattr(self, "_capture_mode", False):
+            self.capture_ready()
+        self._check_points(points)
+        if normals and self.dim != 3:
+            raise TypeError("normals need 3-d points")
+        out = {}
+        if knn:
+            out["indices"] = self._new((self.n, int(k)), np.int32)
+            out["counts"] = self._new((self.n,), np.int32)
+        if normals:
+            out["normals"] = self._new((self.n, 3), self.dtype)
+
+        def issue(stream):
+            N.call("pptkg_forest_rebuild", self._h, N.ptr(points), stream, where="Forest.capture_pipeline()")
+            if knn:
+                N.call("pptkg_forest_knn", self._h, int(k), float(np.float32(dmax)), int(bool(exclude_self)),
+                       self._mem, N.ptr(out["indices"]), N.ptr(out["counts"]), stream,
+                       where="Forest.capture_pipeline()")
+            if normals:
+                N.call("pptkg_forest_normals", self._h, int(k), ctypes.c_float(float(np.float32(r))), 1,
+                       PRECISIONS[precision], self._mem, N.ptr(out["normals"]), None, None, stream,
+                       where="Forest.capture_pipeline()")
+
+        return self._capture(issue), out
+
     # ------------------------------------------------------ graph capture --
     def _capture(self, issue):
-        """Captures issue(stream) -- one native forest query into fixed output
-        tensors -- into a CUDA graph.  The query runs once uncaptured first
-        (it sets up the forest's slot tables and loads the kernels)."""
+        """Captures issue(stream) -- native forest calls into fixed output
+        tensors -- into a CUDA graph.  The calls run once uncaptured first
+        (they set up the forest's slot tables and load the kernels)."""
         import torch
         if not self._torch:
             raise ValueError("graph capture needs a forest built from CUDA tensors")
@@ -231,4 +304,7 @@ class CapturedQuery:
         code = int(self.sink.item())
         if code:
             self.sink.zero_()
+            if code in (20, 21):
+                raise RuntimeError("captured forest rebuild: the points need a deeper tree than planned "
+                                   f"(code {code}; build the forest again)")
             raise RuntimeError(f"captured forest query: device check failed (code {code})")

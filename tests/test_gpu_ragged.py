@@ -164,3 +164,120 @@ def test_autotuned_settings_give_identical_results(gpu):
         N.tune_set("lane_span", 1024)
         N.tune_set("warm_bound", 1)
         N.tune_set("topk_min", 0)
+
+
+def _same_forest(f, g):
+    """Two forests over the same rows hold the same trees and answer alike."""
+    import torch
+    assert np.array_equal(f.valid_offsets, g.valid_offsets)
+    assert np.array_equal(f.reverse_indices(), g.reverse_indices())
+    for c in range(f.ncloud):
+        assert np.array_equal(f.ref_nodes(c), g.ref_nodes(c)), c
+    fi, fc = f.knn(8)
+    gi, gc = g.knn(8)
+    assert torch.equal(fi, gi) and torch.equal(fc, gc)
+    fn, gn = f.normals(8), g.normals(8)
+    assert torch.equal(torch.nan_to_num(fn, nan=-9.0), torch.nan_to_num(gn, nan=-9.0))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_rebuild_equals_a_fresh_forest(gpu, dtype):
+    # capture mode: the trees rebuilt in place from new coordinates of the
+    # same rows (dropped rows moved, clouds squeezed and stretched) are the
+    # trees a new forest builds
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=21, count=30, dtype=dtype)
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    f.capture_ready()
+    rng = np.random.default_rng(3)
+    for trial in range(3):
+        Q = P * rng.uniform(0.5, 2.0, size=(1, 3)).astype(dtype) + rng.normal(size=P.shape).astype(dtype) * 0.01
+        Q[rng.integers(0, len(Q), 50)] = np.nan
+        if trial == 2:
+            Q = P.copy()
+        dq = torch.from_numpy(Q).cuda()
+        f.rebuild(dq)
+        _same_forest(f, ragged.Forest(dq, off))
+
+
+def test_captured_build_and_queries_replay(gpu):
+    # one graph: rebuild from a fixed input tensor, kNN, normals; each
+    # replay after a refill equals a new forest over the refilled points
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=22, count=25)
+    buf = torch.from_numpy(P).cuda()
+    f = ragged.Forest(buf, off)
+    cap, out = f.capture_pipeline(buf, 8)
+    rng = np.random.default_rng(4)
+    for trial in range(3):
+        Q = P + rng.normal(size=P.shape).astype(np.float32) * 0.05
+        Q[rng.integers(0, len(Q), 20)] = np.nan
+        buf.copy_(torch.from_numpy(Q))
+        for t in out.values():
+            t.fill_(-7)
+        cap.replay()
+        torch.cuda.synchronize()
+        cap.check()
+        g = ragged.Forest(torch.from_numpy(Q).cuda(), off)
+        gi, gc = g.knn(8)
+        assert torch.equal(out["indices"], gi) and torch.equal(out["counts"], gc), trial
+        assert torch.equal(torch.nan_to_num(out["normals"], nan=-9.0), torch.nan_to_num(g.normals(8), nan=-9.0))
+        f.refresh()
+        assert np.array_equal(f.valid_offsets, g.valid_offsets)
+
+
+def _chain_cloud(n_clusters=60, per=400, seed=0):
+    """Clusters at x = 2^-j: every widest-axis midpoint split peels off one
+    cluster, so segments above the per-CTA subtree size last ~50 levels."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for j in range(n_clusters):
+        c = rng.normal(size=(per, 3)) * (1e-3 * 2.0 ** -j)
+        c[:, 0] += 2.0 ** -j
+        parts.append(c)
+    return np.concatenate(parts).astype(np.float32)
+
+
+def test_rebuild_deeper_than_planned_is_refused(gpu):
+    import torch
+    from pptk_b200 import ragged
+    deep = _chain_cloud()
+    n = len(deep)
+    P = np.random.default_rng(1).random((n, 3), dtype=np.float32)
+    off = np.array([0, n])
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    f.capture_ready()
+    with pytest.raises(NotImplementedError, match="more tree levels"):
+        f.rebuild(torch.from_numpy(deep).cuda())
+    # the same points through a captured pipeline: the status word says so
+    buf = torch.from_numpy(P).cuda()
+    g = ragged.Forest(buf, off)
+    cap, _ = g.capture_pipeline(buf, 8, normals=False)
+    buf.copy_(torch.from_numpy(deep))
+    cap.replay()
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match="deeper tree"):
+        cap.check()
+    # a new forest over those points is fine
+    h = ragged.Forest(torch.from_numpy(deep).cuda(), off)
+    assert h.n_valid == n
+
+
+def test_rebuild_argument_checks(gpu):
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=23, count=5)
+    f = ragged.Forest(torch.from_numpy(P).cuda(), off)
+    with pytest.raises(ValueError):
+        f.rebuild(torch.from_numpy(P).cuda())  # not capture-ready
+    f.capture_ready()
+    with pytest.raises(ValueError):
+        f.rebuild(torch.from_numpy(P[:-1]).cuda())
+    with pytest.raises(ValueError):
+        f.rebuild(torch.from_numpy(P.astype(np.float64)).cuda())
+    with pytest.raises(TypeError):
+        f.rebuild(P)
+    with pytest.raises(ValueError):
+        ragged.Forest(P, off).capture_ready()
