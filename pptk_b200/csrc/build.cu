@@ -260,15 +260,16 @@ __global__ void k_tiles(Seg<T, D>* segs, int lvl, int* tile_seg, BuildCtl* ctl) 
   }
 }
 
+// The tiles of a level are walked grid-stride by a grid of a few blocks per
+// SM, so a level with few tiles (or none: the trailing levels of a
+// capture-mode rebuild) costs a few hundred idle blocks, not one per tile of
+// the largest level.
 template <typename T, int D>
-__device__ __forceinline__ bool tile_range(const Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, int& s,
-                                           int& start, int& end) {
-  int t = blockIdx.x;
-  if (t >= ctl->n_tiles) return false;
+__device__ __forceinline__ void tile_at(const Seg<T, D>* segs, const int* tile_seg, int t, int& s, int& start,
+                                        int& end) {
   s = tile_seg[t];
   start = segs[s].b + (t - segs[s].tile0) * TILE;
   end = min(start + TILE, segs[s].e);
-  return true;
 }
 
 template <typename T, int D>
@@ -299,43 +300,47 @@ __device__ __forceinline__ T warp_max(T v) {
 
 template <typename T, int D>
 __global__ void __launch_bounds__(BT) k_bbox(Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, SoA<T, D> soa) {
-  int s, start, end;
-  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
   __shared__ T shmn[D][BT / 32], shmx[D][BT / 32];
-  T mn[D], mx[D];
-#pragma unroll
-  for (int d = 0; d < D; d++) {
-    mn[d] = Limits<T>::max();
-    mx[d] = Limits<T>::lowest();
-  }
-  for (int i = start + threadIdx.x; i < end; i += BT) {
+  const int ntiles = ctl->n_tiles;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int s, start, end;
+    tile_at(segs, tile_seg, t, s, start, end);
+    T mn[D], mx[D];
 #pragma unroll
     for (int d = 0; d < D; d++) {
-      T v = soa.x[d][i];
-      mn[d] = min(mn[d], v);
-      mx[d] = max(mx[d], v);
+      mn[d] = Limits<T>::max();
+      mx[d] = Limits<T>::lowest();
     }
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = start + threadIdx.x; i < end; i += BT) {
 #pragma unroll
-  for (int d = 0; d < D; d++) {
-    mn[d] = warp_min(mn[d]);
-    mx[d] = warp_max(mx[d]);
-    if (lane == 0) {
-      shmn[d][wid] = mn[d];
-      shmx[d][wid] = mx[d];
+      for (int d = 0; d < D; d++) {
+        T v = soa.x[d][i];
+        mn[d] = min(mn[d], v);
+        mx[d] = max(mx[d], v);
+      }
     }
-  }
-  __syncthreads();
-  if (threadIdx.x < D) {
-    int d = threadIdx.x;
-    T a = shmn[d][0], b = shmx[d][0];
-    for (int w = 1; w < BT / 32; w++) {
-      a = min(a, shmn[d][w]);
-      b = max(b, shmx[d][w]);
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      mn[d] = warp_min(mn[d]);
+      mx[d] = warp_max(mx[d]);
+      if (lane == 0) {
+        shmn[d][wid] = mn[d];
+        shmx[d][wid] = mx[d];
+      }
     }
-    atomicMin(&segs[s].tlo[d], ord_t<T>(a));
-    atomicMax(&segs[s].thi[d], ord_t<T>(b));
+    __syncthreads();
+    if (threadIdx.x < D) {
+      int d = threadIdx.x;
+      T a = shmn[d][0], b = shmx[d][0];
+      for (int w = 1; w < BT / 32; w++) {
+        a = min(a, shmn[d][w]);
+        b = max(b, shmx[d][w]);
+      }
+      atomicMin(&segs[s].tlo[d], ord_t<T>(a));
+      atomicMax(&segs[s].thi[d], ord_t<T>(b));
+    }
+    __syncthreads();
   }
 }
 
@@ -385,23 +390,26 @@ __global__ void k_node(Seg<T, D>* segs, int lvl, BuildCtl* ctl, Rec<T, D>* recs,
 
 template <typename T, int D>
 __global__ void __launch_bounds__(BT) k_count(Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl, SoA<T, D> soa) {
-  int s, start, end;
-  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
-  if (!segs[s].act) return;
   __shared__ long long sh[33];
-  const T sv = segs[s].sv;
-  const T* v = soa.x[segs[s].sd];
-  int c1 = 0, c2 = 0;
-  for (int i = start + threadIdx.x; i < end; i += BT) {
-    T x = v[i];
-    c1 += x < sv;
-    c2 += x <= sv;
-  }
-  long long packed = ((long long)c2 << 32) | (long long)c1;
-  long long tot = block_sum(packed, sh);
-  if (threadIdx.x == 0) {
-    atomicAdd(&segs[s].L1, (int)(tot & 0xffffffffll));
-    atomicAdd(&segs[s].L2, (int)(tot >> 32));
+  const int ntiles = ctl->n_tiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int s, start, end;
+    tile_at(segs, tile_seg, t, s, start, end);
+    if (!segs[s].act) continue;  // (uniform over the block)
+    const T sv = segs[s].sv;
+    const T* v = soa.x[segs[s].sd];
+    int c1 = 0, c2 = 0;
+    for (int i = start + threadIdx.x; i < end; i += BT) {
+      T x = v[i];
+      c1 += x < sv;
+      c2 += x <= sv;
+    }
+    long long packed = ((long long)c2 << 32) | (long long)c1;
+    long long tot = block_sum(packed, sh);
+    if (threadIdx.x == 0) {
+      atomicAdd(&segs[s].L1, (int)(tot & 0xffffffffll));
+      atomicAdd(&segs[s].L2, (int)(tot >> 32));
+    }
   }
 }
 
@@ -422,83 +430,91 @@ __device__ __forceinline__ void pass_flags(int pass, int i, T x, T sv, int b, in
 template <typename T, int D>
 __global__ void __launch_bounds__(BT) k_flags(int pass, Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl,
                                               SoA<T, D> soa, long long* tile_cnt) {
-  int s, start, end;
-  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
   __shared__ long long sh[33];
-  long long c = 0;
-  if (segs[s].act) {
-    const T sv = segs[s].sv;
-    const T* v = soa.x[segs[s].sd];
-    const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2;
-    for (int i = start + threadIdx.x; i < end; i += BT) {
-      bool bl, gr;
-      pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
-      c += (long long)bl + ((long long)gr << 32);
+  const int ntiles = ctl->n_tiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int s, start, end;
+    tile_at(segs, tile_seg, t, s, start, end);
+    long long c = 0;
+    if (segs[s].act) {
+      const T sv = segs[s].sv;
+      const T* v = soa.x[segs[s].sd];
+      const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2;
+      for (int i = start + threadIdx.x; i < end; i += BT) {
+        bool bl, gr;
+        pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
+        c += (long long)bl + ((long long)gr << 32);
+      }
     }
+    long long tot = block_sum(c, sh);
+    if (threadIdx.x == 0) tile_cnt[t] = tot;
   }
-  long long tot = block_sum(c, sh);
-  if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
 }
 
 template <typename T, int D>
 __global__ void k_tscan(Seg<T, D>* segs, int lvl, const long long* tile_cnt, long long* tile_off, BuildCtl* ctl) {
   __shared__ long long sh[33];
-  if ((int)blockIdx.x >= ctl->level_cnt[lvl]) return;
-  Seg<T, D>& g = segs[blockIdx.x];
-  if (!g.act) return;
-  long long carry = 0;
-  for (int c0 = 0; c0 < g.ntiles; c0 += blockDim.x) {
-    int t = c0 + threadIdx.x;
-    long long v = t < g.ntiles ? tile_cnt[g.tile0 + t] : 0;
-    long long tot;
-    long long ex = block_excl_scan(v, sh, tot);
-    if (t < g.ntiles) tile_off[g.tile0 + t] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) {
-    int nbl = (int)(carry & 0xffffffffll), ngr = (int)(carry >> 32);
-    g.G = nbl;
-    if (nbl != ngr) atomicExch(&ctl->status, 1);
+  const int nseg = ctl->level_cnt[lvl];
+  for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
+    Seg<T, D>& g = segs[si];
+    if (!g.act) continue;  // (uniform over the block)
+    long long carry = 0;
+    for (int c0 = 0; c0 < g.ntiles; c0 += blockDim.x) {
+      int t = c0 + threadIdx.x;
+      long long v = t < g.ntiles ? tile_cnt[g.tile0 + t] : 0;
+      long long tot;
+      long long ex = block_excl_scan(v, sh, tot);
+      if (t < g.ntiles) tile_off[g.tile0 + t] = carry + ex;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) {
+      int nbl = (int)(carry & 0xffffffffll), ngr = (int)(carry >> 32);
+      g.G = nbl;
+      if (nbl != ngr) atomicExch(&ctl->status, 1);
+    }
   }
 }
 
 template <typename T, int D>
 __global__ void __launch_bounds__(BT) k_scatter(int pass, Seg<T, D>* segs, const int* tile_seg, const BuildCtl* ctl,
                                                 SoA<T, D> soa, const long long* tile_off, int* blpos, int* grpos) {
-  int s, start, end;
-  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
-  if (!segs[s].act) return;
   __shared__ long long sh[33];
-  const T sv = segs[s].sv;
-  const T* v = soa.x[segs[s].sd];
-  const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2, G = segs[s].G;
-  const int i0 = start + threadIdx.x * TITEMS;
-  unsigned mbl = 0, mgr = 0;
+  const int ntiles = ctl->n_tiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int s, start, end;
+    tile_at(segs, tile_seg, t, s, start, end);
+    if (!segs[s].act) continue;  // (uniform over the block)
+    const T sv = segs[s].sv;
+    const T* v = soa.x[segs[s].sd];
+    const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2, G = segs[s].G;
+    const int i0 = start + threadIdx.x * TITEMS;
+    unsigned mbl = 0, mgr = 0;
 #pragma unroll
-  for (int j = 0; j < TITEMS; j++) {
-    int i = i0 + j;
-    if (i < end) {
-      bool bl, gr;
-      pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
-      mbl |= (unsigned)bl << j;
-      mgr |= (unsigned)gr << j;
+    for (int j = 0; j < TITEMS; j++) {
+      int i = i0 + j;
+      if (i < end) {
+        bool bl, gr;
+        pass_flags(pass, i, v[i], sv, b, L1, L2, bl, gr);
+        mbl |= (unsigned)bl << j;
+        mgr |= (unsigned)gr << j;
+      }
     }
-  }
-  long long mine = (long long)__popc(mbl) + ((long long)__popc(mgr) << 32);
-  long long tot;
-  long long ex = block_excl_scan(mine, sh, tot) + tile_off[blockIdx.x];
-  int rb = (int)(ex & 0xffffffffll), rg = (int)(ex >> 32);
-  const int size = segs[s].e - b;
+    long long mine = (long long)__popc(mbl) + ((long long)__popc(mgr) << 32);
+    long long tot;
+    long long ex = block_excl_scan(mine, sh, tot) + tile_off[t];
+    int rb = (int)(ex & 0xffffffffll), rg = (int)(ex >> 32);
+    const int size = segs[s].e - b;
 #pragma unroll
-  for (int j = 0; j < TITEMS; j++) {
-    if (mbl >> j & 1) {
-      if (rb < size) blpos[b + rb] = i0 + j;
-      rb++;
-    }
-    if (mgr >> j & 1) {
-      const int slot = G - 1 - rg;
-      if (slot >= 0 && slot < size) grpos[b + slot] = i0 + j;
-      rg++;
+    for (int j = 0; j < TITEMS; j++) {
+      if (mbl >> j & 1) {
+        if (rb < size) blpos[b + rb] = i0 + j;
+        rb++;
+      }
+      if (mgr >> j & 1) {
+        const int slot = G - 1 - rg;
+        if (slot >= 0 && slot < size) grpos[b + slot] = i0 + j;
+        rg++;
+      }
     }
   }
 }
@@ -506,27 +522,30 @@ __global__ void __launch_bounds__(BT) k_scatter(int pass, Seg<T, D>* segs, const
 template <typename T, int D>
 __global__ void __launch_bounds__(BT) k_swap(Seg<T, D>* segs, const int* tile_seg, BuildCtl* ctl, SoA<T, D> soa,
                                              const int* blpos, const int* grpos) {
-  int s, start, end;
-  if (!tile_range(segs, tile_seg, ctl, s, start, end)) return;
-  if (!segs[s].act) return;
-  const int b = segs[s].b, e = segs[s].e, G = segs[s].G;
-  for (int i = start + threadIdx.x; i < end; i += BT) {
-    int j = i - b;
-    if (j >= G) break;
-    int x = blpos[b + j], y = grpos[b + j];
-    if (x < b || x >= e || y < b || y >= e) {
-      atomicExch(&ctl->status, 4);
-      continue;
-    }
+  const int ntiles = ctl->n_tiles;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int s, start, end;
+    tile_at(segs, tile_seg, t, s, start, end);
+    if (!segs[s].act) continue;
+    const int b = segs[s].b, e = segs[s].e, G = segs[s].G;
+    for (int i = start + threadIdx.x; i < end; i += BT) {
+      int j = i - b;
+      if (j >= G) break;
+      int x = blpos[b + j], y = grpos[b + j];
+      if (x < b || x >= e || y < b || y >= e) {
+        atomicExch(&ctl->status, 4);
+        continue;
+      }
 #pragma unroll
-    for (int d = 0; d < D; d++) {
-      T t = soa.x[d][x];
-      soa.x[d][x] = soa.x[d][y];
-      soa.x[d][y] = t;
+      for (int d = 0; d < D; d++) {
+        T tmp = soa.x[d][x];
+        soa.x[d][x] = soa.x[d][y];
+        soa.x[d][y] = tmp;
+      }
+      int tmp = soa.id[x];
+      soa.id[x] = soa.id[y];
+      soa.id[y] = tmp;
     }
-    int t = soa.id[x];
-    soa.id[x] = soa.id[y];
-    soa.id[y] = t;
   }
 }
 
@@ -582,7 +601,10 @@ constexpr int SUB_THREADS = 256;
 
 // Finishes small segments' whole subtrees in shared memory, one warp per
 // node, level by level.  Persistent: each CTA takes segments from the small
-// list until it is exhausted.
+// list until it is exhausted.  (Splitting the first levels' few nodes with
+// the whole block instead was measured slower: a third more subtree time on
+// a 4,096-cloud forest; the warps of the SM's other CTAs already fill the
+// issue slots those levels leave idle.)
 template <typename T, int D>
 __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small, SoA<T, D> soa, Rec<T, D>* recs,
                                                          int* root_rec, int cap_pts, int cap_list, int max_leaf,
@@ -892,6 +914,13 @@ __global__ void k_troots(const Rec<T, D>* recs, const int* root_rec, const int64
 }
 
 // ------------------------------------------------------------ host side ----
+// Grid of the grid-stride level kernels: eight 256-thread blocks per SM.
+static int level_grid(int device) {
+  int nsm = 148;
+  PPTKG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  return std::max(nsm, 1) * 8;
+}
+
 template <typename T, int D>
 int small_capacity(int max_leaf, int& cap_list, size_t& smem) {
   const size_t budget = 72 * 1024;
@@ -1062,7 +1091,8 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
       BuildBuf<int> blpos(nv + 1, st), grpos(nv + 1, st);
       BuildBuf<int> tile_seg(max_tiles, st);
       BuildBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
-      const unsigned gt = (unsigned)max_tiles;
+      const unsigned gt = (unsigned)std::min(max_tiles, level_grid(tree->device));
+      const unsigned gq = (unsigned)std::min(seg_cap, level_grid(tree->device));
       const unsigned gs = (unsigned)div_up(seg_cap, 128);
       int h0 = 0;
       if (nv > 0) {
@@ -1085,7 +1115,7 @@ TreeBase* build_forest(const T* d_in, int64_t n, const int64_t* orig_off_h, int 
         for (int pass = 1; pass <= 2; pass++) {
           k_flags<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_cnt.get());
           PPTKG_CHECK_LAUNCH();
-          k_tscan<T, D><<<(unsigned)seg_cap, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
+          k_tscan<T, D><<<gq, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
           PPTKG_CHECK_LAUNCH();
           k_scatter<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_off.get(), blpos.get(),
                                             grpos.get());
@@ -1343,7 +1373,8 @@ void rebuild_forest(TreeBase* t, const T* d_in, cudaStream_t st, int* status) {
     BuildBuf<int> blpos(n + 1, st), grpos(n + 1, st);
     BuildBuf<int> tile_seg(max_tiles, st);
     BuildBuf<long long> tile_cnt(max_tiles, st), tile_off(max_tiles, st);
-    const unsigned gt = (unsigned)max_tiles;
+    const unsigned gt = (unsigned)std::min(max_tiles, level_grid(t->device));
+    const unsigned gq = (unsigned)std::min(seg_cap, level_grid(t->device));
     const unsigned gs = (unsigned)div_up(seg_cap, 128);
     for (int lvl = 0; lvl < t->cap_levels; lvl++) {
       Seg<T, D>* A = segL[lvl & 1].get();
@@ -1361,7 +1392,7 @@ void rebuild_forest(TreeBase* t, const T* d_in, cudaStream_t st, int* status) {
       for (int pass = 1; pass <= 2; pass++) {
         k_flags<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_cnt.get());
         PPTKG_CHECK_LAUNCH();
-        k_tscan<T, D><<<(unsigned)seg_cap, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
+        k_tscan<T, D><<<gq, 256, 0, st>>>(A, lvl, tile_cnt.get(), tile_off.get(), ctl.get());
         PPTKG_CHECK_LAUNCH();
         k_scatter<T, D><<<gt, BT, 0, st>>>(pass, A, tile_seg.get(), ctl.get(), soa, tile_off.get(), blpos.get(),
                                           grpos.get());

@@ -268,7 +268,7 @@ def test_rebuild_deeper_than_planned_is_refused(gpu):
 def test_rebuild_argument_checks(gpu):
     import torch
     from pptk_b200 import ragged
-    P, off, _ = small_batch(seed=23, count=5)
+    P, off, _ = small_batch(seed=23, count=10)
     f = ragged.Forest(torch.from_numpy(P).cuda(), off)
     with pytest.raises(ValueError):
         f.rebuild(torch.from_numpy(P).cuda())  # not capture-ready
