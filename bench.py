@@ -442,7 +442,7 @@ def run_ragged_workload(args, ctx):
     """Ragged batch: 4,096 clouds (synth.ragged_clouds, seed 4, sizes
     log-uniform in [1k, 200k]); one step builds every cloud's tree in one
     forest build and answers kNN k=16 and normals k=16 for every point of
-    every cloud.  Bucket size, lane_span, warm_bound and topk_min are picked by the autotuner on
+    every cloud.  Bucket size, lane_span, warm_bound, topk_min and warm_mult are picked by the autotuner on
     the first 256 clouds before timing."""
     torch = ctx.torch
     from pptk_b200 import autotune, ragged, synth
@@ -496,6 +496,29 @@ def run_ragged_workload(args, ctx):
                        and torch.equal(torch.nan_to_num(outs["normals"], nan=-9.0),
                                        torch.nan_to_num(f.normals(k), nan=-9.0)))
     del cap_p, outs, ref_i, ref_c
+    # the same comparison on a small batch (512 clouds of 500-5,000
+    # points), where launches and host round trips weigh more
+    Ps, offs = synth.ragged_clouds(512, lo=500, hi=5000, seed=7)
+    devs = torch.from_numpy(Ps).cuda()
+
+    def step_small():
+        fsm = ragged.Forest(devs, offs)
+        fsm.set_bucket(tuned["bucket"])
+        fsm.knn(k)
+        fsm.normals(k)
+
+    for _ in range(args.warmup):
+        step_small()
+    ms_sd, _, _ = device_timed(ctx, step_small, max(args.steps, 10))
+    fsm = ragged.Forest(devs, offs)
+    fsm.set_bucket(tuned["bucket"])
+    bufs = devs.clone()
+    cap_s, outs_s = fsm.capture_pipeline(bufs, k)
+    ms_sg, _, _ = device_timed(ctx, cap_s.replay, max(args.steps, 10))
+    cap_s.check()
+    ri, rc = fsm.knn(k)
+    small_ok = bool(torch.equal(outs_s["indices"], ri) and torch.equal(outs_s["counts"], rc))
+    del cap_s, outs_s, fsm, bufs, devs
     e2e = None
     if not args.no_e2e:
         host = torch.from_numpy(P).pin_memory().numpy()
@@ -517,6 +540,7 @@ def run_ragged_workload(args, ctx):
                        "parallelism": f"replicas x{ctx.world}"},
             "autotune": {"bucket": tuned["bucket"], "lane_span": tuned["lane_span"],
                          "warm_bound": tuned.get("warm_bound"), "topk_min": tuned.get("topk_min"),
+                         "warm_mult": tuned.get("warm_mult"),
                          "sample": "first 256 clouds", "table": tuned["table"],
                          "knob_table": tuned.get("knob_table")},
             "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
@@ -525,6 +549,8 @@ def run_ragged_workload(args, ctx):
             "graph_pipeline": {"value": ctx.world * n / (ctx.max_over_ranks(ms_p) / 1e3), "unit": "points/s",
                                "ms_per_step": ms_p, "direct_ms_per_step": ms_max, "equal_to_direct": pipeline_ok,
                                "kernels_in_graph": kernels_p,
+                               "small_batch": {"clouds": 512, "points": int(len(Ps)), "ms_per_step": ms_sg,
+                                               "direct_ms_per_step": ms_sd, "equal_to_direct": small_ok},
                                "what": "the whole step (forest rebuild + kNN + normals) replayed from one CUDA "
                                        "graph on a capture-ready forest"},
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof,
@@ -1033,6 +1059,8 @@ def run_config(name, args, ctx):
         gp = res["graph_pipeline"]
         summary["graph_step_ms"] = round(gp["ms_per_step"], 1)
         summary["graph_step_equal"] = gp["equal_to_direct"]
+        summary["graph_vs_direct_small_ms"] = [round(gp["small_batch"]["ms_per_step"], 2),
+                                               round(gp["small_batch"]["direct_ms_per_step"], 2)]
         summary["e2e_value"] = (res["e2e"] or {}).get("value")
     elif name == "multitree":
         lq, lh = _lat(res["latency"]), _lat(res["latency_at_half_load"])

@@ -1,6 +1,6 @@
 """Autotuner for the traversal settings of a workload.
 
-Four settings shape every kNN / normal traversal; none changes a result:
+Five settings shape every kNN / normal traversal; none changes a result:
 
 * the leaf bucket size of the traversal hierarchy (``set_bucket`` on a tree
   or forest): larger buckets mean fewer node visits and more candidates;
@@ -10,7 +10,10 @@ Four settings shape every kNN / normal traversal; none changes a result:
 * ``warm_bound``: whether the warm-started lists also take the seed bound of
   a wider window of tree-order neighbours;
 * ``topk_min``: the k-tiling of the register top-k lists (their compile-time
-  capacity, at least the smallest of 4/8/16/32/64 that holds k).
+  capacity, at least the smallest of 4/8/16/32/64 that holds k);
+* ``warm_mult``: the width of the warm-start window of full-capacity float
+  lists, in multiples of k (2 is best for queries in tree order; 3 was
+  faster for scattered kNN queries on the 20M scene).
 
 ``tune`` times a caller-supplied workload on a sample: the full grid of
 bucket x lane_span first, then one pass over each further knob with the
@@ -23,7 +26,7 @@ from . import _native as N
 
 BUCKETS = (16, 32, 64, 128)
 LANE_SPANS = (-1, 64, 256, 1024)
-EXTRA_KNOBS = {"warm_bound": (0, 1), "topk_min": (0, 32)}
+EXTRA_KNOBS = {"warm_bound": (0, 1), "topk_min": (0, 32), "warm_mult": (2, 3)}
 
 
 def _time(run, sync, repeats):

@@ -242,6 +242,13 @@ class Server:
         results: smaller batches let one batch's host copies overlap another
         batch's kernels.
 
+    defer_ms: while a normal-slot batch is running, another normal slot
+        starts a batch only once at least min_batch_queries queries wait or
+        the oldest waiting request has waited defer_ms (0: start at once).
+        Under steady arrivals this folds the requests that arrive during a
+        batch into the next one instead of a string of small batches, which
+        run at a lower query rate (less coherent query packets, fixed costs
+        per batch).
     trace: keep, for every batch, CUDA events recorded on its stream before
         and after its work (``trace`` list of (kinds, fast slot, start,
         end)), so that the device-side overlap of batches can be checked.
@@ -255,7 +262,7 @@ class Server:
 
     def __init__(self, budget_bytes=150e9, slots=3, device=0, max_batch_queries=20_000_000, engine=None,
                  fast_slots=1, small_batch=65_536, max_host_batch_queries=8_000_000, batch_ms=None,
-                 min_batch_queries=1_000_000, trace=False):
+                 min_batch_queries=1_000_000, trace=False, defer_ms=0.0):
         self.budget = float(budget_bytes)
         self.engine = engine or GpuEngine(device)
         self.max_batch = int(max_batch_queries)
@@ -263,6 +270,8 @@ class Server:
         self.small_batch = int(small_batch)
         self.batch_ms = None if batch_ms is None else float(batch_ms)
         self.min_batch = int(min_batch_queries)
+        self.defer_s = max(0.0, float(defer_ms)) / 1e3
+        self._normal_running = 0
         self._rate = None  # queries per second of recent batches (EMA)
         self.trace = [] if trace else None
         self.trees = {}
@@ -421,8 +430,11 @@ class Server:
                 if not self._free:
                     continue
                 batch, slot = [], None
+                defer = self._defer()
                 # a fast slot first when small requests wait, then the others
                 for i in sorted(range(len(self._free)), key=lambda j: not self._free[j][1]):
+                    if defer and not self._free[i][1]:
+                        continue
                     batch = self._admit(self._free[i][1])
                     if batch:
                         slot = self._free.pop(i)
@@ -431,7 +443,25 @@ class Server:
                     self._cv.wait(0.001)
                     continue
                 self._batches += 1
+                if not slot[1]:
+                    self._normal_running += 1
             self._pool.submit(self._run, batch, slot)
+
+    def _defer(self):
+        """True while a new normal-slot batch should wait (see defer_ms)."""
+        if self.defer_s <= 0 or self._normal_running == 0 or not self._queue:
+            return False
+        waiting = 0
+        oldest = None
+        for r in self._queue:
+            if r.kind in ("knn", "normals"):
+                waiting += r.m - r.next_row
+                oldest = r.t_submit if oldest is None else min(oldest, r.t_submit)
+            else:
+                return False  # builds and r-near run at once
+        if waiting >= self.min_batch or oldest is None:
+            return False
+        return time.perf_counter() - oldest < self.defer_s
 
     def _run(self, batch, slot):
         stream = slot[0]
@@ -489,6 +519,8 @@ class Server:
             with self._cv:
                 for sl in batch:
                     self._committed -= sl.r.bytes * sl.m / max(sl.r.m, 1) if sl.r.m else sl.r.bytes
+                if not slot[1]:
+                    self._normal_running -= 1
                 self._free.append(slot)
                 self._cv.notify_all()
 

@@ -149,21 +149,25 @@ def test_autotuned_settings_give_identical_results(gpu):
     try:
         res = autotune.tune(lambda: f.knn(8), f.set_bucket, buckets=(16, 64), lane_spans=(-1, 0), repeats=1)
         assert res["bucket"] in (16, 64) and res["lane_span"] in (-1, 0) and len(res["table"]) == 4
-        assert res["warm_bound"] in (0, 1) and res["topk_min"] in (0, 32) and len(res["knob_table"]) == 4
-        for b, ls, wb, tk in ((16, -1, 1, 0), (64, 0, 0, 32), (64, 256, 1, 16),
-                              (res["bucket"], res["lane_span"], res["warm_bound"], res["topk_min"])):
+        assert res["warm_bound"] in (0, 1) and res["topk_min"] in (0, 32) and res["warm_mult"] in (2, 3)
+        assert len(res["knob_table"]) == 6
+        for b, ls, wb, tk, wm in ((16, -1, 1, 0, 2), (64, 0, 0, 32, 3), (64, 256, 1, 16, 4), (32, 1024, 1, 8, 1),
+                                  (res["bucket"], res["lane_span"], res["warm_bound"], res["topk_min"],
+                                   res["warm_mult"])):
             f.set_bucket(b)
             N.tune_set("lane_span", ls)
             N.tune_set("warm_bound", wb)
             N.tune_set("topk_min", tk)
+            N.tune_set("warm_mult", wm)
             i, c = f.knn(8)
-            assert torch.equal(i, ref_i) and torch.equal(c, ref_c), (b, ls, wb, tk)
+            assert torch.equal(i, ref_i) and torch.equal(c, ref_c), (b, ls, wb, tk, wm)
             n = f.normals(8)
-            assert torch.equal(torch.nan_to_num(n, nan=-9.0), torch.nan_to_num(ref_n, nan=-9.0)), (b, ls, wb, tk)
+            assert torch.equal(torch.nan_to_num(n, nan=-9.0), torch.nan_to_num(ref_n, nan=-9.0)), (b, ls, wb, tk, wm)
     finally:
         N.tune_set("lane_span", 1024)
         N.tune_set("warm_bound", 1)
         N.tune_set("topk_min", 0)
+        N.tune_set("warm_mult", 2)
 
 
 def _same_forest(f, g):

@@ -249,3 +249,45 @@ def test_batch_cap_follows_the_measured_rate():
     srv._rate = 1e4
     assert srv.batch_cap() == 1000  # never below the lower bound
     srv.close()
+
+
+def test_deferred_batches_fold_the_requests_that_arrive_during_a_batch():
+    # while one normal-slot batch runs, the other normal slot waits for
+    # min_batch_queries queued queries (or defer_ms) instead of starting a
+    # small batch; the requests then run together
+    eng = FakeEngine(delay=0.2)
+    srv = serving.Server(budget_bytes=1e9, slots=3, fast_slots=1, engine=eng, small_batch=4,
+                         min_batch_queries=100, defer_ms=5_000)
+    rng = np.random.default_rng(6)
+    pts = rng.random((100, 3))
+    tid = srv.build(pts).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((10, 3)), k=2)
+    wait_started(eng, "knn")
+    qs = [rng.random((20, 3)) for _ in range(2)]
+    futs = [srv.knn(tid, q, k=2) for q in qs]
+    blocker.result(timeout=10)
+    for q, f in zip(qs, futs):
+        idx, _ = f.result(timeout=10)
+        d = ((q[:, None, :] - pts[None]) ** 2).sum(-1)
+        assert np.array_equal(idx, np.argsort(d, axis=1, kind="stable")[:, :2])
+    with eng.lock:
+        knn = [b for b in eng.batches if b[0] == "knn"]
+    assert len(knn) == 2 and knn[1][1] == 2  # the blocker, then both requests in one launch
+    srv.close()
+
+
+def test_deferral_ends_after_defer_ms():
+    eng = FakeEngine(delay=1.0)
+    srv = serving.Server(budget_bytes=1e9, slots=3, fast_slots=1, engine=eng, small_batch=4,
+                         min_batch_queries=100, defer_ms=50)
+    rng = np.random.default_rng(7)
+    tid = srv.build(rng.random((50, 3))).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((10, 3)), k=2)
+    wait_started(eng, "knn")
+    t0 = time.perf_counter()
+    late = srv.knn(tid, rng.random((20, 3)), k=2)
+    wait_started(eng, "knn", count=2, timeout=0.8)  # starts while the blocker still runs
+    assert time.perf_counter() - t0 >= 0.04
+    assert not blocker.done()
+    late.result(timeout=10)
+    srv.close()
