@@ -67,6 +67,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "kNN+normal queries/s at k=16 on 20M pts (plain vs batched/serving); p50/p99 lat"
 BYTES_PER_QUERY = 216  # 3*4 query + 16*3*4 neighbours + 3*4 normal (f32, indices not materialised)
+# one walk for the self kNN and the normal (k=16, f32): 3*4 query + 16*(3*4 + 4) neighbours read,
+# 16*4 indices + 4 count + 3*4 normal written
+BYTES_PER_QUERY_FUSED = 12 + 16 * 16 + 64 + 4 + 12
 
 
 def parse():
@@ -370,19 +373,20 @@ def device_timed(ctx, fn, steps):
 TRAFFIC_PER_QUERY = {"tree_order": 126.8, "scattered": 160.5}
 
 
-def roofline(ctx, stage_name, queries, traffic_kind):
+def roofline(ctx, stage_name, queries, traffic_kind, bytes_per_query=BYTES_PER_QUERY):
+    """traffic_kind None: no ncu traffic figure for this kernel's launch."""
     peak, peak_kind = load_peaks()
     t_ms, cnt = ctx.stage(stage_name)
     if not cnt or t_ms <= 0:
         return None
     per_launch_ms = t_ms / cnt
-    bytes_per_launch = BYTES_PER_QUERY * queries / cnt
+    bytes_per_launch = bytes_per_query * queries / cnt
     achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
-    traffic = TRAFFIC_PER_QUERY[traffic_kind] * queries / cnt
+    traffic = TRAFFIC_PER_QUERY[traffic_kind] * queries / cnt if traffic_kind else None
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": "k_normals", "peak_kind": f"{peak_kind} hbm_gbs",
             "ms_per_launch": per_launch_ms, "bytes_per_launch": bytes_per_launch,
-            "traffic_source": f"ncu bytes/query ({traffic_kind}) x queries"}
+            "traffic_source": f"ncu bytes/query ({traffic_kind}) x queries" if traffic_kind else None}
 
 
 BUILD_STAGES = ("build", "build.prep", "build.attempt", "build.levels", "build.subtree", "build.finish",
@@ -442,8 +446,10 @@ def run_ragged_workload(args, ctx):
     """Ragged batch: 4,096 clouds (synth.ragged_clouds, seed 4, sizes
     log-uniform in [1k, 200k]); one step builds every cloud's tree in one
     forest build and answers kNN k=16 and normals k=16 for every point of
-    every cloud.  Bucket size, lane_span, warm_bound, topk_min and warm_mult are picked by the autotuner on
-    the first 256 clouds before timing."""
+    every cloud -- one Forest.knn_normals traversal per point (the same
+    results as Forest.knn + Forest.normals, which are timed beside it).
+    Bucket size, lane_span, warm_bound, topk_min and warm_mult are picked by
+    the autotuner on the first 256 clouds before timing."""
     torch = ctx.torch
     from pptk_b200 import autotune, ragged, synth
     k = args.k
@@ -452,10 +458,15 @@ def run_ragged_workload(args, ctx):
     dev = torch.from_numpy(P).cuda()
     sample_end = int(off[256])
     fs = ragged.Forest(dev[:sample_end], off[:257])
-    tuned = autotune.tune(lambda: (fs.knn(k), fs.normals(k)), fs.set_bucket)
+    tuned = autotune.tune(lambda: fs.knn_normals(k), fs.set_bucket)
     del fs
 
     def step():
+        f = ragged.Forest(dev, off)
+        f.set_bucket(tuned["bucket"])
+        f.knn_normals(k)
+
+    def step_separate():
         f = ragged.Forest(dev, off)
         f.set_bucket(tuned["bucket"])
         f.knn(k)
@@ -466,13 +477,21 @@ def run_ragged_workload(args, ctx):
     ctx.lib.pptkg_profile_enable(1)
     ms, launches, clk = device_timed(ctx, step, args.steps)
     stages = {}
-    for nm in BUILD_STAGES[:7] + ("forest.knn", "forest.normals"):
+    for nm in BUILD_STAGES[:7] + ("forest.knn_normals",):
         t_, c_ = ctx.stage(nm)
         stages[nm] = {"ms_per_step": t_ / args.steps, "calls_per_step": c_ / args.steps}
-    roof = roofline(ctx, "forest.normals", n * args.steps, "tree_order")
+    roof = roofline(ctx, "forest.knn_normals", n * args.steps, None, BYTES_PER_QUERY_FUSED)
     ctx.lib.pptkg_profile_enable(0)
     ms_max = ctx.max_over_ranks(ms)
     value = ctx.throughput(n, ms / 1e3)
+    # the same step as two calls (Forest.knn, then Forest.normals)
+    step_separate()
+    ctx.lib.pptkg_profile_enable(1)
+    ms_sep, _, _ = device_timed(ctx, step_separate, args.steps)
+    for nm in ("forest.knn", "forest.normals"):
+        t_, c_ = ctx.stage(nm)
+        stages[nm + " (separate calls)"] = {"ms_per_step": t_ / args.steps, "calls_per_step": c_ / args.steps}
+    ctx.lib.pptkg_profile_enable(0)
     # the same queries replayed from CUDA graphs on a built forest
     f = ragged.Forest(dev, off)
     f.set_bucket(tuned["bucket"])
@@ -504,8 +523,7 @@ def run_ragged_workload(args, ctx):
     def step_small():
         fsm = ragged.Forest(devs, offs)
         fsm.set_bucket(tuned["bucket"])
-        fsm.knn(k)
-        fsm.normals(k)
+        fsm.knn_normals(k)
 
     for _ in range(args.warmup):
         step_small()
@@ -528,8 +546,7 @@ def run_ragged_workload(args, ctx):
         for _ in range(args.steps):
             fh = ragged.Forest(host, off)
             fh.set_bucket(tuned["bucket"])
-            i, c = fh.knn(k)
-            nn = fh.normals(k)
+            i, c, nn = fh.knn_normals(k)
         dt = ctx.max_over_ranks((time.perf_counter() - t0) / args.steps)
         e2e = {"value": ctx.world * n / dt, "unit": "queries/s", "h2d_bytes_per_step": int(P.nbytes),
                "d2h_bytes_per_step": int(i.nbytes + c.nbytes + nn.nbytes)}
@@ -543,6 +560,8 @@ def run_ragged_workload(args, ctx):
                          "warm_mult": tuned.get("warm_mult"),
                          "sample": "first 256 clouds", "table": tuned["table"],
                          "knob_table": tuned.get("knob_table")},
+            "separate_calls": {"ms_per_step": ms_sep, "what": "the same step with Forest.knn and Forest.normals "
+                                                             "as two traversals"},
             "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
                              "ms_per_step": ms_q, "what": "kNN + normals of every point, replayed from two CUDA "
                                                          "graphs on the built forest"},
@@ -551,7 +570,7 @@ def run_ragged_workload(args, ctx):
                                "kernels_in_graph": kernels_p,
                                "small_batch": {"clouds": 512, "points": int(len(Ps)), "ms_per_step": ms_sg,
                                                "direct_ms_per_step": ms_sd, "equal_to_direct": small_ok},
-                               "what": "the whole step (forest rebuild + kNN + normals) replayed from one CUDA "
+                               "what": "the whole step (forest rebuild + one kNN + normals traversal) replayed from one CUDA "
                                        "graph on a capture-ready forest"},
             "e2e": e2e, "gpu_launches": launches, "stages_ms": stages, "roofline": roof,
             "cpu_baseline": None, "clocks": clk}
@@ -1054,7 +1073,8 @@ def run_config(name, args, ctx):
     elif name == "ragged":
         st = res["stages_ms"]
         summary["stage_ms"] = {k: round(v["ms_per_step"], 1) for k, v in st.items()
-                               if k in ("build", "forest.knn", "forest.normals")}
+                               if k in ("build", "forest.knn_normals")}
+        summary["separate_calls_ms"] = round(res["separate_calls"]["ms_per_step"], 1)
         summary["graph_replay_queries_ms"] = round(res["graph_replay"]["ms_per_step"], 1)
         gp = res["graph_pipeline"]
         summary["graph_step_ms"] = round(gp["ms_per_step"], 1)

@@ -210,6 +210,15 @@ PPTKG_API int pptkg_forest_knn(const pptkg_tree* forest, int k, double dmax, int
 PPTKG_API int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
                                    void* out_evecs, void* out_evals, int32_t* out_sizes, void* stream);
 
+/* Self kNN and PCA normals of every point in one walk (no reference
+ * counterpart; the reference answers them with two calls): equal to
+ * pptkg_forest_knn(k, dmax = r, exclude_self = 1) into out_idx / out_cnt
+ * and pptkg_forest_normals(k, r, ...) into out_evecs / out_evals /
+ * out_sizes.  out_cnt, out_evals and out_sizes may be NULL. */
+PPTKG_API int pptkg_forest_knn_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision,
+                                       int mem, int32_t* out_idx, int32_t* out_cnt, void* out_evecs,
+                                       void* out_evals, int32_t* out_sizes, void* stream);
+
 /* Capture mode of a float32 / float64 forest (no reference counterpart; the
  * rebuild step of a CUDA graph over build and queries).
  * pptkg_forest_capture_ready sizes the forest's device arrays for new
@@ -312,8 +321,9 @@ PPTKG_API int pptkg_tune_get(const char* name, int64_t* value);
 
 /* Status sink of the calling host thread (no reference counterpart; for
  * capturing forest queries into a CUDA graph).  While d_word (a device int,
- * or NULL to clear) is set, pptkg_forest_knn / pptkg_forest_normals with
- * device buffers record kernel check failures by writing a non-zero code
+ * or NULL to clear) is set, pptkg_forest_knn / pptkg_forest_normals /
+ * pptkg_forest_knn_normals / pptkg_forest_rebuild with device buffers
+ * record kernel check failures by writing a non-zero code
  * into *d_word and neither synchronise nor read it back; the caller zeroes
  * the word and checks it after the work (or a graph replay) completes.  A
  * forest's first query sets up device tables and must run without a sink. */

@@ -60,6 +60,7 @@ SIGNATURES = {
     "pptkg_forest_ref_nodes": [_vp, _int, _vp, _i64, _pi64],
     "pptkg_forest_knn": [_vp, _int, _dbl, _int, _int, _vp, _vp, _vp],
     "pptkg_forest_normals": [_vp, _int, _flt, _int, _int, _int, _vp, _vp, _vp, _vp],
+    "pptkg_forest_knn_normals": [_vp, _int, _flt, _int, _int, _int, _vp, _vp, _vp, _vp, _vp, _vp],
     "pptkg_forest_capture_ready": [_vp, _vp],
     "pptkg_forest_rebuild": [_vp, _vp, _vp],
     "pptkg_tree_normals_noalloc": [_vp, _vp, _i64, _int, _flt, _int, _int, _vp, _vp, _vp, _vp],

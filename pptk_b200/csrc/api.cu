@@ -448,6 +448,33 @@ int pptkg_forest_normals(const pptkg_tree* forest, int k, float r, int num_eigen
   });
 }
 
+int pptkg_forest_knn_normals(const pptkg_tree* forest, int k, float r, int num_eigen, int precision, int mem,
+                             int32_t* out_idx, int32_t* out_cnt, void* out_evecs, void* out_evals,
+                             int32_t* out_sizes, void* stream) {
+  return guarded([&] {
+    const TreeBase* t = tree_raw(forest);
+    DeviceGuard g(t->device);
+    if (num_eigen != 1 && num_eigen != 3) throw Error(E_INVALID, "num_eigen must be 1 or 3");
+    if (!(r > 0.0f)) throw Error(E_INVALID, "r must be positive");
+    if (t->n && !out_idx) throw Error(E_INVALID, "out_idx is null");
+    dispatch_float(t->dtype, [&](auto tt) {
+      typedef decltype(tt) T;
+      Staged<int32_t> oi(out_idx, (size_t)t->n * k, mem, false, S(stream));
+      Staged<int32_t> oc(out_cnt, (size_t)t->n, mem, false, S(stream));
+      Staged<T> ev(out_evecs, (size_t)t->n * 3 * num_eigen, mem, false, S(stream));
+      Staged<T> ew(out_evals, (size_t)t->n * num_eigen, mem, false, S(stream));
+      Staged<int32_t> sz(out_sizes, (size_t)t->n, mem, false, S(stream));
+      forest_normals<T>(t, k, r, num_eigen, precision, DEFAULT_GAP, ev.d, ew.d, sz.d, S(stream), oi.d, oc.d);
+      oi.flush(S(stream));
+      oc.flush(S(stream));
+      ev.flush(S(stream));
+      ew.flush(S(stream));
+      sz.flush(S(stream));
+      if (!(g_status_sink && mem == PPTKG_MEM_DEVICE)) PPTKG_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+  });
+}
+
 static std::vector<const TreeBase*> tree_list(const pptkg_tree* const* trees, int ntrees) {
   if (ntrees < 1 || !trees) throw Error(E_INVALID, "need at least one tree");
   std::vector<const TreeBase*> v(ntrees);

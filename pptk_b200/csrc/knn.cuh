@@ -134,6 +134,10 @@ struct TopK<KMAX, float> {
   __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return s[j] < lim && (unsigned)s[j] != 0xffffffffu; }
   __device__ __forceinline__ int id(int j) const { return (int)(unsigned)(s[j] & 0xffffffffull); }
+  // Slot j sorts before the key (0, id0) of a point at distance 0.
+  __device__ __forceinline__ bool below_zero(int j, int id0) const {
+    return s[j] < (unsigned long long)(unsigned)id0;
+  }
   __device__ __forceinline__ float dist(int j) const { return __uint_as_float((unsigned)(s[j] >> 32)); }
   // Warm start (see warm_topk): slot j holds a real candidate, an empty
   // live slot (no candidate yet) or a dead slot (beyond k); sort_desc()
@@ -220,6 +224,7 @@ struct TopK<KMAX, double> {
   __device__ __forceinline__ void reserve(int) {}
   __device__ __forceinline__ bool valid(int j) const { return p[j] >= 0 && p[j] != 0x7fffffff && d[j] >= 0.0; }
   __device__ __forceinline__ int id(int j) const { return p[j]; }
+  __device__ __forceinline__ bool below_zero(int j, int id0) const { return d[j] == 0.0 && p[j] < id0; }
   __device__ __forceinline__ double dist(int j) const { return d[j]; }
   __device__ __forceinline__ void set_real(int j, double d2, int id) {
     d[j] = d2;

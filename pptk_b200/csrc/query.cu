@@ -1077,13 +1077,22 @@ constexpr int normals_min_blocks(int kmax, int dist_bytes, int prec) {
 // Fused kNN + PCA.  In the FP32 precision mode a neighbourhood whose two
 // smallest eigenvalues nearly coincide (relative gap < gap_thr) is queued in
 // `fix` for an FP64 re-solve by a second launch of this kernel in FP64 mode.
+//
+// With knn_idx set (forest queries with a loader that excludes the query
+// point, own), one walk answers both a self kNN and the normal: the list is
+// the k nearest other points, written to knn_idx / knn_cnt as k_knn writes
+// them, and the neighbourhood of the normal is that list with the query
+// point put in at its place in (dist2, id) order and cut to k -- the k
+// nearest including the query point, in the order the normal-only walk
+// gathers them, so both results equal the separate calls.
 template <typename T, int KMAX, typename L, int PREC>
 __global__ void __launch_bounds__(QTHREADS, normals_min_blocks(KMAX, sizeof(typename DistOf<T>::type), PREC))
 k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
                                                       int k, typename DistOf<T>::type r2, int num_eigen,
                                                       double gap_thr, T* evecs, T* evals, int32_t* sizes,
                                                       int* fix, int* nfix, int* status, SlotMap fm, int lane_span,
-                                                      bool warm_bound, int warm_mult) {
+                                                      bool warm_bound, int warm_mult, int32_t* knn_idx,
+                                                      int32_t* knn_cnt) {
   typedef typename DistOf<T>::type DistT;
   constexpr int LOGCAP = normals_logcap(KMAX);
   const int slot = blockIdx.x * QTHREADS + threadIdx.x;
@@ -1114,14 +1123,40 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   if (qid < 0) return;
   if (!active) {
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
+    if (knn_idx) {
+      for (int j = 0; j < k; j++) knn_idx[(int64_t)qid * k + j] = -1;
+      if (knn_cnt) knn_cnt[qid] = 0;
+    }
     return;
   }
   // the list holds point ids; the neighbours are gathered from their tree
   // positions (the index map's loads are independent and overlap)
   int n = 0;
+  if (knn_idx) {
+    int c = 0;
+    bool placed = false;
 #pragma unroll
-  for (int j = KMAX - 1; j >= 0; j--)
-    if (j < k && top.valid(j)) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
+    for (int j = KMAX - 1; j >= 0; j--) {
+      if (j < k) {
+        const bool v = top.valid(j);
+        knn_idx[(int64_t)qid * k + (k - 1 - j)] = v ? top.id(j) : -1;
+        if (v) {
+          c++;
+          if (!placed && !top.below_zero(j, qid)) {
+            lane_log[(n++) * 32] = own;
+            placed = true;
+          }
+          if (n < k) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
+        }
+      }
+    }
+    if (!placed && n < k) lane_log[(n++) * 32] = own;
+    if (knn_cnt) knn_cnt[qid] = c;
+  } else {
+#pragma unroll
+    for (int j = KMAX - 1; j >= 0; j--)
+      if (j < k && top.valid(j)) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
+  }
   if (PREC == PREC_FP64) {
     Sym3<double> C = log_covariance<T, double, DistT>(tv, lane_log, n, q);
     double w[3], V[9];
@@ -1325,7 +1360,7 @@ __global__ void k_refine64(const PointRec<T, 3>* pts, const int* fix, const int*
 template <typename T, int KMAX, typename L, int PREC>
 void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                     int num_eigen, double gap_thr, T* ev, T* ew, int32_t* sz, int* fix, int* nfix, int* status,
-                    cudaStream_t st, SlotMap fm = SlotMap{}) {
+                    cudaStream_t st, SlotMap fm = SlotMap{}, int32_t* kidx = nullptr, int32_t* kcnt = nullptr) {
   if (m <= 0) return;
   const size_t smem = QWARPS * warp_smem_bytes<T, 3>(t->tdepth, normals_logcap(KMAX));
   if (smem > 48 * 1024)
@@ -1333,24 +1368,24 @@ void launch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, 
         cudaFuncSetAttribute(k_normals<T, KMAX, L, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_normals<T, KMAX, L, PREC><<<div_up(m, QTHREADS), QTHREADS, smem, st>>>(
       view_of<T, 3>(t), ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix, nfix, status, fm,
-      g_tune_lane_span.load(), g_tune_warm_bound.load() != 0, g_tune_warm_mult.load());
+      g_tune_lane_span.load(), g_tune_warm_bound.load() != 0, g_tune_warm_mult.load(), kidx, kcnt);
   PPTKG_CHECK_LAUNCH();
 }
 
 template <typename T, int KMAX, typename L>
 void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, int k, typename DistOf<T>::type r2,
                   int num_eigen, int prec, double gap_thr, T* ev, T* ew, int32_t* sz, int* status, cudaStream_t st,
-                  SlotMap fm = SlotMap{}) {
+                  SlotMap fm = SlotMap{}, int32_t* kidx = nullptr, int32_t* kcnt = nullptr) {
   if (prec == PREC_FP64) {
     launch_normals<T, KMAX, L, PREC_FP64>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, nullptr,
-                                          nullptr, status, st, fm);
+                                          nullptr, status, st, fm, kidx, kcnt);
     return;
   }
   // FP32 pass, then an FP64 re-solve of the queued small-gap neighbourhoods
   DevBuf<int> fix((size_t)std::max(m, 1) * (KMAX + 2), st), nfix(1, st);
   PPTKG_CUDA(cudaMemsetAsync(nfix.get(), 0, sizeof(int), st));
   launch_normals<T, KMAX, L, PREC_FP32>(t, ld, order, mode, m, k, r2, num_eigen, gap_thr, ev, ew, sz, fix.get(),
-                                        nfix.get(), status, st, fm);
+                                        nfix.get(), status, st, fm, kidx, kcnt);
   {
     Stage s("normals.refine64", st);
     k_refine64<T, KMAX><<<div_up(m, 256), 256, 0, st>>>((const PointRec<T, 3>*)t->pts, fix.get(), nfix.get(),
@@ -1363,18 +1398,24 @@ void normals_pass(const TreeBase* t, L ld, const int* order, int mode, int m, in
 template <typename T, typename L>
 void dispatch_normals(const TreeBase* t, L ld, const int* order, int mode, int m, int k,
                       typename DistOf<T>::type r2, int num_eigen, int prec, double gap_thr, T* ev, T* ew,
-                      int32_t* sz, int* status, cudaStream_t st, SlotMap fm = SlotMap{}) {
+                      int32_t* sz, int* status, cudaStream_t st, SlotMap fm = SlotMap{}, int32_t* kidx = nullptr,
+                      int32_t* kcnt = nullptr) {
   const int kc = std::max(k, g_tune_topk_min.load());
   if (kc <= 4)
-    normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
+    normals_pass<T, 4, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm, kidx,
+                          kcnt);
   else if (kc <= 8)
-    normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
+    normals_pass<T, 8, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm, kidx,
+                          kcnt);
   else if (kc <= 16)
-    normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
+    normals_pass<T, 16, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm, kidx,
+                           kcnt);
   else if (kc <= 32)
-    normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
+    normals_pass<T, 32, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm, kidx,
+                           kcnt);
   else
-    normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm);
+    normals_pass<T, 64, L>(t, ld, order, mode, m, k, r2, num_eigen, prec, gap_thr, ev, ew, sz, status, st, fm, kidx,
+                           kcnt);
 }
 
 // Normals of neighbourhoods held as tree positions (pos: m x k, counts cnt),
@@ -1639,7 +1680,7 @@ __global__ void k_fill_invalid(int64_t n, int num_eigen, T* evecs, T* evals, int
 
 template <typename T>
 void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
-                    T* d_evals, int32_t* d_sizes, cudaStream_t st) {
+                    T* d_evals, int32_t* d_sizes, cudaStream_t st, int32_t* d_idx, int32_t* d_cnt) {
   typedef typename DistOf<T>::type DistT;
   if (t->dim != 3) throw Error(E_TYPE, "normals need 3-d points");
   if (k < 1) throw Error(E_INVALID, "forest normals need k >= 1");
@@ -1651,12 +1692,25 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
   if ((t->capture || t->n > t->nv) && t->n > 0) {
     k_fill_invalid<T><<<(unsigned)((t->n + 255) / 256), 256, 0, st>>>(t->n, num_eigen, d_evecs, d_evals, d_sizes);
     PPTKG_CHECK_LAUNCH();
+    // (and no neighbours, for the fused kNN)
+    if (d_idx) PPTKG_CUDA(cudaMemsetAsync(d_idx, 0xff, sizeof(int32_t) * (size_t)t->n * k, st));
+    if (d_cnt) PPTKG_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int32_t) * (size_t)t->n, st));
   }
   if (n_slots == 0) return;
   StatusWord status(st);
   const DistT rr = (DistT)(T)r;
   const DistT r2 = rr * rr;
   int prec = precision == PREC_AUTO ? (sizeof(T) == 4 ? PREC_FP32 : PREC_FP64) : precision;
+  if (d_idx) {
+    // one walk for the self kNN (the list excludes the query point) and
+    // the normal (the query point put back in)
+    Stage stage("forest.knn_normals", st);
+    dispatch_normals<T, IndexQueries<3, true>>(t, IndexQueries<3, true>{nullptr, t->fwd}, nullptr, 0, (int)n_slots,
+                                               k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals, d_sizes,
+                                               status.get(), st, fm, d_idx, d_cnt);
+    status.check(st, "forest kNN + normals");
+    return;
+  }
   Stage stage("forest.normals", st);
   dispatch_normals<T, IndexQueries<3, false>>(t, IndexQueries<3, false>{nullptr, t->fwd}, nullptr, 0, (int)n_slots,
                                               k, r2, num_eigen, prec, gap_thr, d_evecs, d_evals, d_sizes, status.get(),
@@ -1668,9 +1722,9 @@ void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precis
 template void forest_knn<float, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
 template void forest_knn<double, 3>(const TreeBase*, int, double, bool, int32_t*, int32_t*, cudaStream_t);
 template void forest_normals<float>(const TreeBase*, int, float, int, int, double, float*, float*, int32_t*,
-                                    cudaStream_t);
+                                    cudaStream_t, int32_t*, int32_t*);
 template void forest_normals<double>(const TreeBase*, int, float, int, int, double, double*, double*, int32_t*,
-                                     cudaStream_t);
+                                     cudaStream_t, int32_t*, int32_t*);
 #endif  // PPTKG_QUERY_DIM
 
 

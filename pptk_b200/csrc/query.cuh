@@ -46,9 +46,13 @@ void normals_query(const TreeBase* t, const QuerySpec& qs, int k, float r, int n
 template <typename T, int D>
 void forest_knn(const TreeBase* t, int k, double dmax, bool exclude_self, int32_t* d_idx, int32_t* d_cnt,
                 cudaStream_t st);
+// With d_idx set, forest_normals also answers the self kNN (k, dmax = r,
+// the point itself excluded) from the same walk: d_idx n x k, d_cnt n, as
+// forest_knn writes them.
 template <typename T>
 void forest_normals(const TreeBase* t, int k, float r, int num_eigen, int precision, double gap_thr, T* d_evecs,
-                    T* d_evals, int32_t* d_sizes, cudaStream_t st);
+                    T* d_evals, int32_t* d_sizes, cudaStream_t st, int32_t* d_idx = nullptr,
+                    int32_t* d_cnt = nullptr);
 
 // Device-side slot map of a capture-ready forest (after each rebuild).
 void forest_slot_map_device(TreeBase* t, cudaStream_t st);

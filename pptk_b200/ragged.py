@@ -165,6 +165,21 @@ class Forest:
             return ev
         return ev, ew, sz
 
+    def knn_normals(self, k, r=math.inf, precision="auto"):
+        """(indices, counts, normals): Forest.knn(k, dmax=r, exclude_self=True)
+        and Forest.normals(k, r) from one traversal per point; each result
+        equals the separate call."""
+        from .estimate_normals import PRECISIONS
+        if self.dim != 3:
+            raise TypeError("normals need 3-d points")
+        idx = self._new((self.n, int(k)), np.int32)
+        cnt = self._new((self.n,), np.int32)
+        ev = self._new((self.n, 3), self.dtype)
+        N.call("pptkg_forest_knn_normals", self._h, int(k), ctypes.c_float(float(np.float32(r))), 1,
+               PRECISIONS[precision], self._mem, N.ptr(idx), N.ptr(cnt), N.ptr(ev), None, None, self._stream,
+               where="Forest.knn_normals()")
+        return idx, cnt, ev
+
     # ------------------------------------------------------- rebuilds --
     def capture_ready(self):
         """Sizes the forest's device arrays for rebuilds from any coordinates
@@ -204,14 +219,16 @@ class Forest:
         self.refresh()
 
     def capture_pipeline(self, points, k, r=math.inf, knn=True, normals=True, dmax=math.inf, exclude_self=True,
-                         precision="auto"):
+                         precision="auto", fused=True):
         """(CapturedQuery, outputs): one CUDA graph that rebuilds the forest
         from `points` (a fixed CUDA tensor the caller refills between
         replays), then runs Forest.knn (k, dmax, exclude_self) and / or
-        Forest.normals (k, r) into fixed tensors.  outputs: {"indices",
-        "counts", "normals"} as requested.  Calls capture_ready() if needed.
-        A replay whose points need a deeper tree than the first build's + 8
-        levels makes check() raise (build a new forest then)."""
+        Forest.normals (k, r) into fixed tensors -- as one Forest.knn_normals
+        traversal when both are asked for with exclude_self and dmax == r
+        (unless fused=False).  outputs: {"indices", "counts", "normals"} as
+        requested.  Calls capture_ready() if needed.  A replay whose points
+        need a deeper tree than the first build's + 8 levels makes check()
+        raise (build a new forest then)."""
         from .estimate_normals import PRECISIONS
         if not getattr(self, "_capture_mode", False):
             self.capture_ready()
@@ -225,8 +242,16 @@ class Forest:
         if normals:
             out["normals"] = self._new((self.n, 3), self.dtype)
 
+        one_walk = (fused and knn and normals and exclude_self
+                    and float(np.float32(dmax)) == float(np.float32(r)))
+
         def issue(stream):
             N.call("pptkg_forest_rebuild", self._h, N.ptr(points), stream, where="Forest.capture_pipeline()")
+            if one_walk:
+                N.call("pptkg_forest_knn_normals", self._h, int(k), ctypes.c_float(float(np.float32(r))), 1,
+                       PRECISIONS[precision], self._mem, N.ptr(out["indices"]), N.ptr(out["counts"]),
+                       N.ptr(out["normals"]), None, None, stream, where="Forest.capture_pipeline()")
+                return
             if knn:
                 N.call("pptkg_forest_knn", self._h, int(k), float(np.float32(dmax)), int(bool(exclude_self)),
                        self._mem, N.ptr(out["indices"]), N.ptr(out["counts"]), stream,

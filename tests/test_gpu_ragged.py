@@ -285,3 +285,48 @@ def test_rebuild_argument_checks(gpu):
         f.rebuild(P)
     with pytest.raises(ValueError):
         ragged.Forest(P, off).capture_ready()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_fused_knn_normals_equal_the_separate_calls(gpu, dtype):
+    # one walk per point answers the self kNN and the normal; with exact
+    # duplicates the query point's place among the zero-distance points
+    # follows the index rule (a cloud of 40 copies of one point, and a cloud
+    # whose first 20 rows repeat one point)
+    import torch
+    from pptk_b200 import ragged
+    P, off, clouds = small_batch(seed=31, count=20, dtype=dtype)
+    rng = np.random.default_rng(5)
+    dup = np.repeat(rng.random((1, 3)), 40, axis=0).astype(dtype)
+    mixed = rng.random((300, 3)).astype(dtype)
+    mixed[:20] = mixed[0]
+    P = np.concatenate([P, dup, mixed])
+    off = np.concatenate([off, [off[-1] + 40, off[-1] + 340]])
+    for dev in (False, True):
+        f = ragged.Forest(torch.from_numpy(P).cuda() if dev else P, off)
+        for k in (4, 16, 24):
+            i2, c2, n2 = f.knn_normals(k)
+            i1, c1 = f.knn(k)
+            n1 = f.normals(k)
+            if dev:
+                i1, c1, n1, i2, c2, n2 = (x.cpu().numpy() for x in (i1, c1, n1, i2, c2, n2))
+            assert np.array_equal(i1, i2) and np.array_equal(c1, c2), (dev, k)
+            assert np.array_equal(np.nan_to_num(n1, nan=-9.0), np.nan_to_num(n2, nan=-9.0)), (dev, k)
+
+
+def test_fused_pipeline_replay_equals_separate_calls(gpu):
+    import torch
+    from pptk_b200 import ragged
+    P, off, _ = small_batch(seed=32, count=25)
+    buf = torch.from_numpy(P).cuda()
+    f = ragged.Forest(buf, off)
+    cap, out = f.capture_pipeline(buf, 16)
+    Q = P + np.random.default_rng(8).normal(size=P.shape).astype(np.float32) * 0.02
+    buf.copy_(torch.from_numpy(Q))
+    cap.replay()
+    torch.cuda.synchronize()
+    cap.check()
+    g = ragged.Forest(torch.from_numpy(Q).cuda(), off)
+    gi, gc = g.knn(16)
+    assert torch.equal(out["indices"], gi) and torch.equal(out["counts"], gc)
+    assert torch.equal(torch.nan_to_num(out["normals"], nan=-9.0), torch.nan_to_num(g.normals(16), nan=-9.0))
