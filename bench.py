@@ -364,6 +364,44 @@ def device_timed(ctx, fn, steps):
     return e0.elapsed_time(e1) / steps, int(launches), clocks.stop()
 
 
+class ResultSink:
+    """Takes a load test's futures as a client would: each answer is checked
+    (and handed to on_result) when it arrives, then dropped, so a latency run
+    keeps no answers alive in HBM -- held to the end, the answers of a
+    6-second run at half load (tens of GB) made every batch allocate new
+    device memory, and those allocations showed up as 100-500 ms stalls."""
+
+    def __init__(self, on_result=None):
+        self.cv = threading.Condition()
+        self.n = 0
+        self.errors = []
+        self.on_result = on_result
+
+    def add(self, fut, tag=None):
+        with self.cv:
+            self.n += 1
+
+        def done(f):
+            try:
+                res = f.result()
+                if self.on_result is not None:
+                    self.on_result(tag, res)
+            except BaseException as e:  # noqa: BLE001 -- reported by wait()
+                self.errors.append(e)
+            with self.cv:
+                self.n -= 1
+                self.cv.notify_all()
+
+        fut.add_done_callback(done)
+
+    def wait(self):
+        with self.cv:
+            while self.n:
+                self.cv.wait(0.1)
+        if self.errors:
+            raise self.errors[0]
+
+
 # DRAM bytes per query of k_normals (k=16, float32) from one ncu capture each
 # (dram__bytes_read.sum + dram__bytes_write.sum of a launch over its
 # queries) on an 8M-point scene: tree-order queries and scattered serving
@@ -492,15 +530,8 @@ def run_ragged_workload(args, ctx):
         t_, c_ = ctx.stage(nm)
         stages[nm + " (separate calls)"] = {"ms_per_step": t_ / args.steps, "calls_per_step": c_ / args.steps}
     ctx.lib.pptkg_profile_enable(0)
-    # the same queries replayed from CUDA graphs on a built forest
     f = ragged.Forest(dev, off)
     f.set_bucket(tuned["bucket"])
-    cap_k, _ = f.capture_knn(k)
-    cap_n, _ = f.capture_normals(k)
-    ms_q, _, _ = device_timed(ctx, lambda: (cap_k.replay(), cap_n.replay()), args.steps)
-    cap_k.check()
-    cap_n.check()
-    del cap_k, cap_n
     # the whole step (forest rebuild from the points + kNN + normals)
     # replayed from one CUDA graph; its results are checked against the
     # direct calls once
@@ -562,9 +593,6 @@ def run_ragged_workload(args, ctx):
                          "knob_table": tuned.get("knob_table")},
             "separate_calls": {"ms_per_step": ms_sep, "what": "the same step with Forest.knn and Forest.normals "
                                                              "as two traversals"},
-            "graph_replay": {"value": ctx.world * n / (ctx.max_over_ranks(ms_q) / 1e3), "unit": "queries/s",
-                             "ms_per_step": ms_q, "what": "kNN + normals of every point, replayed from two CUDA "
-                                                         "graphs on the built forest"},
             "graph_pipeline": {"value": ctx.world * n / (ctx.max_over_ranks(ms_p) / 1e3), "unit": "points/s",
                                "ms_per_step": ms_p, "direct_ms_per_step": ms_max, "equal_to_direct": pipeline_ok,
                                "kernels_in_graph": kernels_p,
@@ -695,16 +723,16 @@ def run_multitree_workload(args, ctx):
         t_start = time.perf_counter()
         nxt = t_start
         pending = []
+        sink = ResultSink(lambda rq, res: built.append(res) if rq[0] == "build" else None)
         for rq in stream_reqs:
             while time.perf_counter() < nxt:
                 time.sleep(max(0.0, min(nxt - time.perf_counter(), 0.002)))
-            pending.append((rq, submit(rq)))
+            sink.add(submit(rq), rq)
+            pending.append((rq, None))
             nxt += arr.exponential(1.0 / rate)
             if time.perf_counter() - t_start > args.latency_seconds:
                 break
-        for i, (rq, f) in enumerate(pending):
-            finish(rq, f)
-            pending[i] = (rq, None)
+        sink.wait()
         span = time.perf_counter() - t_start
         drop_built()
         st = srv.stats(since=t_start)
@@ -867,7 +895,7 @@ def run_serving_workload(args, ctx):
         offered = frac * per_step / (ms_max / 1e3)
         mean_m = per_step / len(mix_dev)
         t_start = time.perf_counter()
-        futs, i = [], 0
+        sink, i = ResultSink(), 0
         next_t = t_start
         while time.perf_counter() - t_start < args.latency_seconds:
             now = time.perf_counter()
@@ -875,11 +903,10 @@ def run_serving_workload(args, ctx):
                 time.sleep(min(next_t - now, 0.002))
                 continue
             kind, a = mix_dev[i % len(mix_dev)]
-            futs.append(srv.knn(tid, a, k=k) if kind == "knn" else srv.normals(tid, a, k=k))
+            sink.add(srv.knn(tid, a, k=k) if kind == "knn" else srv.normals(tid, a, k=k))
             i += 1
             next_t += rng.exponential(mean_m / offered)
-        for f in futs:
-            f.result()
+        sink.wait()
         st = srv.stats(since=t_start)
         with srv._cv:
             lat_all = [d[3] - d[2] for d in srv._done if d[2] >= t_start and d[0] in ("knn", "normals")]
@@ -1075,7 +1102,6 @@ def run_config(name, args, ctx):
         summary["stage_ms"] = {k: round(v["ms_per_step"], 1) for k, v in st.items()
                                if k in ("build", "forest.knn_normals")}
         summary["separate_calls_ms"] = round(res["separate_calls"]["ms_per_step"], 1)
-        summary["graph_replay_queries_ms"] = round(res["graph_replay"]["ms_per_step"], 1)
         gp = res["graph_pipeline"]
         summary["graph_step_ms"] = round(gp["ms_per_step"], 1)
         summary["graph_step_equal"] = gp["equal_to_direct"]
