@@ -64,6 +64,14 @@ typedef struct pptkg_tree pptkg_tree;
 /* Library version (major * 10000 + minor * 100 + patch). */
 PPTKG_API int pptkg_version(void);
 
+/* 1 for the diagnostic build compiled with PPTKG_BOUNDS_CHECK
+ * (libpptkg_checked.so), 0 otherwise.  In that build every point-record,
+ * index-map and traversal-node index the query kernels read is checked
+ * against its array; a failed check records its site in a device word and
+ * reads element 0 instead, and the call returns PPTKG_E_DEVICE ("bounds
+ * check failed: ...").  Traversal stack depths are checked in every build. */
+PPTKG_API int pptkg_bounds_checked(void);
+
 /* Copies the last error message of this thread into buf (NUL-terminated,
  * truncated to len); returns the status of that error. */
 PPTKG_API int pptkg_last_error(char* buf, size_t len);

@@ -18,6 +18,10 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OBJ = os.path.join(PKG, "_lib", "obj")
 LIB = os.path.join(PKG, "_lib", "libpptkg.so")
+# the diagnostic build with every tree index of the query kernels checked
+# (-DPPTKG_BOUNDS_CHECK); load it with PPTKG_LIBRARY=<path>
+OBJ_CHECKED = os.path.join(PKG, "_lib", "obj_checked")
+LIB_CHECKED = os.path.join(PKG, "_lib", "libpptkg_checked.so")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -61,15 +65,19 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False, extra_flags=()):
-    """Compiles the library if any source changed; returns its path."""
-    os.makedirs(OBJ, exist_ok=True)
+def build(force=False, verbose=False, extra_flags=(), bounds_check=False):
+    """Compiles the library if any source changed; returns its path.
+    bounds_check: the PPTKG_BOUNDS_CHECK build into libpptkg_checked.so."""
+    obj_dir, lib_path = (OBJ_CHECKED, LIB_CHECKED) if bounds_check else (OBJ, LIB)
+    if bounds_check:
+        extra_flags = (*extra_flags, "-DPPTKG_BOUNDS_CHECK")
+    os.makedirs(obj_dir, exist_ok=True)
     srcs = _sources()
     hdrs = _headers()
     cc = nvcc()
     jobs = []
     for s in srcs:
-        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(obj_dir, os.path.basename(s)[:-3] + ".o")
         if force or _stale(o, [s] + _included_sources(s) + hdrs + [__file__]):
             jobs.append((s, o))
 
@@ -88,14 +96,14 @@ def build(force=False, verbose=False, extra_flags=()):
             for msg in ex.map(compile_one, jobs):
                 if verbose and msg:
                     print(msg)
-    objs = [os.path.join(OBJ, os.path.basename(s)[:-3] + ".o") for s in srcs]
-    if force or jobs or _stale(LIB, objs):
-        cmd = [cc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB + ".tmp",
+    objs = [os.path.join(obj_dir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    if force or jobs or _stale(lib_path, objs):
+        cmd = [cc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", lib_path + ".tmp",
                "-Xcompiler", "-fPIC"]
         subprocess.check_call(cmd)
-        os.replace(LIB + ".tmp", LIB)
-    return LIB
+        os.replace(lib_path + ".tmp", lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, bounds_check="--bounds-check" in sys.argv))

@@ -9,7 +9,10 @@ import threading
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libpptkg.so")
+# PPTKG_LIBRARY selects another build of the library (the bounds-checked
+# diagnostic build, libpptkg_checked.so)
+LIB_PATH = os.environ.get("PPTKG_LIBRARY") or os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib",
+                                                            "libpptkg.so")
 
 OK, E_INVALID, E_TYPE, E_CUDA, E_RANGE, E_DEVICE, E_UNSUPPORTED = range(7)
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -40,6 +43,7 @@ _pint = ctypes.POINTER(ctypes.c_int)
 
 SIGNATURES = {
     "pptkg_version": [],
+    "pptkg_bounds_checked": [],
     "pptkg_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "pptkg_tree_build": [_vp, _i64, _int, _int, _int, _int, _dbl, _vp, _pvp],
     "pptkg_tree_free": [_vp],

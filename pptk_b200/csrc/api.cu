@@ -28,6 +28,18 @@ int guarded(F&& f) {
   try {
     keep_pool_cached(0);
     f();
+#ifdef PPTKG_BOUNDS_CHECK
+    // index checks of the query kernels (not while a status sink is set:
+    // reading the word would synchronise a capture)
+    if (!g_status_sink) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      static const char* const kSite[] = {"", "point record", "index map", "traversal node"};
+      if (const int site = bounds_take(dev))
+        throw Error(E_DEVICE, std::string("bounds check failed: ") +
+                                  (site > 0 && site < 4 ? kSite[site] : "unknown") + " index out of range");
+    }
+#endif
     return PPTKG_OK;
   } catch (const Error& e) {
     g_msg = e.what();
@@ -292,6 +304,14 @@ extern "C" {
 static int ref_nodes(const pptkg_tree* tree, int cloud, double* out, int64_t capacity, int64_t* count);
 
 int pptkg_version(void) { return 100; }
+
+int pptkg_bounds_checked(void) {
+#ifdef PPTKG_BOUNDS_CHECK
+  return 1;
+#else
+  return 0;
+#endif
+}
 
 int pptkg_last_error(char* buf, size_t len) {
   if (buf && len) {

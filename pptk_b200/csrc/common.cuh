@@ -68,6 +68,14 @@ extern std::atomic<int> g_tune_warm_mult;
 // neither synchronise nor read it back, so their launches can be captured
 // into a CUDA graph.
 extern thread_local int* g_status_sink;
+
+// PPTKG_BOUNDS_CHECK builds: the device word (one per device) where the
+// query kernels' index checks record the first failing site (TreeView::
+// checked), and its read-and-clear; in the normal build bounds_word is null
+// and bounds_take 0.
+int* bounds_word(int device);
+int bounds_take(int device);
+
 #define PPTKG_CHECK_LAUNCH()          \
   do {                                \
     ::pptkg::g_launches++;            \

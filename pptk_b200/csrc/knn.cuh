@@ -365,7 +365,7 @@ __device__ __forceinline__ bool packet_walk(const TreeView<T, D>& tv, const Dist
     }
     sp++;
   };
-  TNode<T, D> nd = load_node(tv.nodes, tv.root);
+  TNode<T, D> nd = load_node(tv.nodes, tv.node_index(tv.root));
   while (true) {
     if (++visits > tv.n_nodes) {  // a tree is acyclic: more visits mean a corrupt node array
       ok = false;
@@ -388,7 +388,7 @@ __device__ __forceinline__ bool packet_walk(const TreeView<T, D>& tv, const Dist
     if (a0 && ref0 >= 0) {
       // near child is an inner node: fetch it now, defer the far child
       next = ref0;
-      nn = load_node(tv.nodes, next);
+      nn = load_node(tv.nodes, tv.node_index(next));
       if (a1) {
         T lo1[D], hi1[D];
 #pragma unroll
@@ -402,7 +402,7 @@ __device__ __forceinline__ bool packet_walk(const TreeView<T, D>& tv, const Dist
       if (a1 && ref1 >= 0) {
         // far child is an inner node: its fetch overlaps the near bucket scan
         next = ref1;
-        nn = load_node(tv.nodes, next);
+        nn = load_node(tv.nodes, tv.node_index(next));
       }
       if (a0) scan(-ref0 - 1, cnt0, m0);
       const bool m1 = need(md1);  // re-test against the tightened threshold
@@ -428,7 +428,7 @@ __device__ __forceinline__ bool packet_walk(const TreeView<T, D>& tv, const Dist
         scan(-e.ref - 1, e.cnt, me);
         continue;
       }
-      nd = load_node(tv.nodes, e.ref);
+      nd = load_node(tv.nodes, tv.node_index(e.ref));
       found = true;
       break;
     }
@@ -468,7 +468,7 @@ __device__ bool packet_knn(const TreeView<T, D>& tv, const DistT* q, int own, bo
       const int nb = min(32, begin + count - base);
       PointRec<T, D> pr;
       if (lane < nb) {
-        pr = tv.pts[base + lane];
+        pr = tv.pt(base + lane);
       } else {
 #pragma unroll
         for (int d = 0; d < D; d++) pr.c[d] = (T)0;
@@ -536,7 +536,7 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
       DistT d2[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        r[j] = tv.pts[p + j];
+        r[j] = tv.pt(p + j);
         d2[j] = point_dist2<T, DistT, D>(r[j].c, q);
       }
 #pragma unroll
@@ -545,7 +545,7 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
           top.offer(d2[j], r[j].id);
     }
     for (; p < end; p++) {
-      const PointRec<T, D> r = tv.pts[p];
+      const PointRec<T, D> r = tv.pt(p);
       const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
       if (d2 <= top.worst() && d2 < r2 && p != own && (unsigned)(p - wlo) >= (unsigned)wn) top.offer(d2, r.id);
     }
@@ -553,7 +553,7 @@ __device__ bool lane_knn(const TreeView<T, D>& tv, const DistT* q, int own, bool
   int cur = tv.root, visits = 0;
   while (true) {
     if (++visits > tv.n_nodes) return false;  // a tree is acyclic: more visits mean a corrupt node array
-    const TNode<T, D> nd = load_node(tv.nodes, cur);
+    const TNode<T, D> nd = load_node(tv.nodes, tv.node_index(cur));
     const DistT md0 = nd.cnt[0] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[0], nd.hi[0], q) : (DistT)INFINITY;
     const DistT md1 = nd.cnt[1] > 0 ? box_min_dist2<T, DistT, D>(nd.lo[1], nd.hi[1], q) : (DistT)INFINITY;
     const bool sw = md1 < md0;
@@ -688,7 +688,7 @@ __device__ bool packet_rnear(const TreeView<T, D>& tv, const DistT* q, bool acti
     for (int base = begin; base < begin + cnt; base += 32) {
       const int nb = min(32, begin + cnt - base);
       __syncwarp();
-      if (lane < nb) ws.buf[lane] = tv.pts[base + lane];
+      if (lane < nb) ws.buf[lane] = tv.pt(base + lane);
       __syncwarp();
       if (mine) {
         for (int t = 0; t < nb; t++) {

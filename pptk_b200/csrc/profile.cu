@@ -21,6 +21,39 @@ std::atomic<int> g_tune_topk_min{0};
 std::atomic<int> g_tune_warm_mult{2};
 thread_local int* g_status_sink = nullptr;
 
+#ifdef PPTKG_BOUNDS_CHECK
+static std::mutex g_bmu;
+static std::map<int, int*> g_bwords;
+int* bounds_word(int device) {
+  std::lock_guard<std::mutex> g(g_bmu);
+  auto it = g_bwords.find(device);
+  if (it != g_bwords.end()) return it->second;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  int* w = nullptr;
+  if (cudaMalloc((void**)&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) w = nullptr;
+  cudaSetDevice(prev);
+  g_bwords[device] = w;
+  return w;
+}
+int bounds_take(int device) {
+  int* w = bounds_word(device);
+  if (!w) return 0;
+  int prev = 0, h = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaDeviceSynchronize();
+  cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost);
+  if (h) cudaMemset(w, 0, sizeof(int));
+  cudaSetDevice(prev);
+  return h;
+}
+#else
+int* bounds_word(int) { return nullptr; }
+int bounds_take(int) { return 0; }
+#endif
+
 namespace {
 struct Pending {
   std::string name;

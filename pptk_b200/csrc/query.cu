@@ -27,6 +27,8 @@ TreeView<T, D> view_of(const TreeBase* t) {
   v.root = t->root_tnode_h.empty() ? 0 : t->root_tnode_h[0];
   v.fwd = t->fwd;
   v.n_in = (int)t->n;
+  v.pts_cap = (int)(t->capture ? t->n : t->nv);
+  v.err = bounds_word(t->device);
   return v;
 }
 
@@ -109,16 +111,23 @@ struct IndexQueries {
       atomicExch(bad, 4);
       return false;
     }
-    const int p = (fwd ? fwd : tv.fwd)[o];
+    const int p = tv.pos_of(fwd ? fwd : tv.fwd, o);
     if (anchor) *anchor = p;
     if (p < 0) return false;  // the point was dropped (NaN/inf): no neighbours
-    const PointRec<T, D> r = tv.pts[p];
+    const PointRec<T, D> r = tv.pt(p);
 #pragma unroll
     for (int d = 0; d < D; d++) out[d] = (DistT)r.c[d];
     own = EXCL ? p : -1;
     return true;
   }
 };
+
+// Loaders whose query point is excluded from its own list (self kNN); with
+// one, k_normals runs its fused form (kNN outputs + the point put back).
+template <typename L>
+struct ExcludesSelf : std::false_type {};
+template <int D>
+struct ExcludesSelf<IndexQueries<D, true>> : std::true_type {};
 
 // Forest queries: every valid point of every cloud, in tree order, each
 // cloud's range padded to whole warps so that a warp never mixes trees.
@@ -149,7 +158,7 @@ __device__ __forceinline__ int forest_query(int slot, const SlotMap& fm, TreeVie
   }
   tv.root = fm.root_tnode[c];
   const int64_t p = fm.valid_off[c] + (slot - fm.slot_off[c]);
-  return p < fm.valid_off[c + 1] ? tv.pts[p].id : -1;
+  return p < fm.valid_off[c + 1] ? tv.pt(p).id : -1;
 }
 
 // Per-lane stack capacity of the per-lane walk (trees deeper than this use
@@ -177,7 +186,7 @@ __device__ __forceinline__ DistT seed_bound(const TreeView<T, D>& tv, const Dist
   DistT m0 = (DistT)0, m1 = (DistT)0, m2 = (DistT)0;
   for (int p = b0; p < b2 + w; p++) {
     if (p == own) continue;
-    const DistT d2 = point_dist2<T, DistT, D>(tv.pts[p].c, q);
+    const DistT d2 = point_dist2<T, DistT, D>(tv.pt(p).c, q);
     if (p < b0 + w) m0 = d2 > m0 ? d2 : m0;
     if (p >= b1 && p < b1 + w) m1 = d2 > m1 ? d2 : m1;
     if (p >= b2) m2 = d2 > m2 ? d2 : m2;
@@ -201,7 +210,7 @@ __device__ __forceinline__ float seed_bound32(const TreeView<T, D>& tv, const fl
 #pragma unroll
   for (int j = 0; j < 32; j++) {
     const int p = b + j;
-    v[j] = (p < hi && p != own) ? point_dist2<T, float, D>(tv.pts[p].c, q) : INFINITY;
+    v[j] = (p < hi && p != own) ? point_dist2<T, float, D>(tv.pt(p).c, q) : INFINITY;
   }
 #pragma unroll
   for (int size = 2; size <= 32; size <<= 1)
@@ -280,7 +289,7 @@ __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, co
       auto key_at = [&](int p) {
         unsigned long long key = top.key_empty();
         if (p < hi && p != own) {
-          const PointRec<T, D> r = tv.pts[p];
+          const PointRec<T, D> r = tv.pt(p);
           const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
           if (d2 < r2) key = top.key_real(d2, r.id);
         }
@@ -320,7 +329,7 @@ __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, co
       else
         top.set_empty(j);
     } else {
-      const PointRec<T, D> r = tv.pts[p];
+      const PointRec<T, D> r = tv.pt(p);
       const DistT d2 = point_dist2<T, DistT, D>(r.c, q);
       if (d2 < r2)
         top.set_real(j, d2, r.id);
@@ -346,7 +355,7 @@ __device__ __forceinline__ void warm_topk(Top& top, const TreeView<T, D>& tv, co
 // original index stored at tree position slot).
 template <typename T, int D>
 __device__ __forceinline__ int query_of(int slot, const int* order, int order_mode, const TreeView<T, D>& tv) {
-  return order_mode == 0 ? slot : (order_mode == 1 ? order[slot] : tv.pts[slot].id);
+  return order_mode == 0 ? slot : (order_mode == 1 ? order[slot] : tv.pt(slot).id);
 }
 
 // ----------------------------------------------------------- ordering ----
@@ -360,7 +369,7 @@ __global__ void k_locate(TreeView<T, D> tv, const Q* q, int m, int* key) {
   for (int d = 0; d < D; d++) p[d] = (DistT)q[(int64_t)i * D + d];
   int cur = tv.root, k = 0;
   for (int step = 0; step <= tv.depth + 1; step++) {
-    const TNode<T, D> nd = load_node(tv.nodes, cur);
+    const TNode<T, D> nd = load_node(tv.nodes, tv.node_index(cur));
     int c;
     if (nd.cnt[1] == 0)
       c = 0;
@@ -610,7 +619,7 @@ __global__ void k_knn_big(TreeView<T, D> tv, L ld, const int* order, int order_m
   top.sort();
   const int64_t row = POS ? i : qid;
   int32_t* out = out_idx + row * k;
-  for (int j = 0; j < k; j++) out[j] = j < top.size ? (POS ? tv.fwd[top.p[j]] : top.p[j]) : -1;
+  for (int j = 0; j < k; j++) out[j] = j < top.size ? (POS ? tv.pos_of(tv.fwd, top.p[j]) : top.p[j]) : -1;
   if (out_cnt) out_cnt[row] = top.size;
 }
 
@@ -777,7 +786,7 @@ __device__ __forceinline__ bool warp_rnear_walk(const TreeView<T, D>& tv, const 
       bad = true;
       break;
     }
-    const TNode<T, D> nd = load_node(tv.nodes, cur);
+    const TNode<T, D> nd = load_node(tv.nodes, tv.node_index(cur));
     const int b1 = b + nd.cnt[0];
     int next = take(nd, 0, b);
     if (next >= 0) {
@@ -808,7 +817,7 @@ __device__ __forceinline__ bool warp_rnear_walk(const TreeView<T, D>& tv, const 
     while (sp > 0 && !bad) {
       --sp;
       const int e = stk[2 * sp], eb = stk[2 * sp + 1];
-      const int r = take(load_node(tv.nodes, e >> 1), e & 1, eb);
+      const int r = take(load_node(tv.nodes, tv.node_index(e >> 1)), e & 1, eb);
       if (r >= 0) {
         cur = r;
         b = eb;
@@ -864,9 +873,9 @@ __global__ void __launch_bounds__(QTHREADS) k_rnear_warp(TreeView<T, D> tv, L ld
       if (p < begin + n) {
         if (whole) {
           hit = p != own;
-          if (hit) id = tv.pts[p].id;
+          if (hit) id = tv.pt(p).id;
         } else {
-          const PointRec<T, D> pr = tv.pts[p];
+          const PointRec<T, D> pr = tv.pt(p);
           hit = point_dist2<T, DistT, D>(pr.c, q) < r2 && (COUNT || p != own);
           id = pr.id;
         }
@@ -1002,7 +1011,7 @@ __device__ __forceinline__ Sym3<P> log_covariance(const TreeView<T, 3>& tv, cons
   typedef typename std::conditional<(sizeof(T) > sizeof(P)), T, P>::type W;
   P s0 = 0, s1 = 0, s2 = 0;
   for (int j = 0; j < n; j++) {
-    const PointRec<T, 3> r = tv.pts[log[j * 32]];
+    const PointRec<T, 3> r = tv.pt(log[j * 32]);
     s0 += (P)((W)r.c[0] - (W)q[0]);
     s1 += (P)((W)r.c[1] - (W)q[1]);
     s2 += (P)((W)r.c[2] - (W)q[2]);
@@ -1011,7 +1020,7 @@ __device__ __forceinline__ Sym3<P> log_covariance(const TreeView<T, 3>& tv, cons
   const P m0 = s0 * inv, m1 = s1 * inv, m2 = s2 * inv;
   CSum<P> c00, c01, c02, c11, c12, c22;
   for (int j = 0; j < n; j++) {
-    const PointRec<T, 3> r = tv.pts[log[j * 32]];
+    const PointRec<T, 3> r = tv.pt(log[j * 32]);
     const P e0 = (P)((W)r.c[0] - (W)q[0]) - m0;
     const P e1 = (P)((W)r.c[1] - (W)q[1]) - m1;
     const P e2 = (P)((W)r.c[2] - (W)q[2]) - m2;
@@ -1078,8 +1087,9 @@ constexpr int normals_min_blocks(int kmax, int dist_bytes, int prec) {
 // smallest eigenvalues nearly coincide (relative gap < gap_thr) is queued in
 // `fix` for an FP64 re-solve by a second launch of this kernel in FP64 mode.
 //
-// With knn_idx set (forest queries with a loader that excludes the query
-// point, own), one walk answers both a self kNN and the normal: the list is
+// With a loader that excludes the query point, own (ExcludesSelf; the
+// forest's fused query, knn_idx set), one walk answers both a self kNN and
+// the normal: the list is
 // the k nearest other points, written to knn_idx / knn_cnt as k_knn writes
 // them, and the neighbourhood of the normal is that list with the query
 // point put in at its place in (dist2, id) order and cut to k -- the k
@@ -1123,7 +1133,7 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   if (qid < 0) return;
   if (!active) {
     write_invalid<T>(qid, num_eigen, evecs, evals, sizes);
-    if (knn_idx) {
+    if constexpr (ExcludesSelf<L>::value) {
       for (int j = 0; j < k; j++) knn_idx[(int64_t)qid * k + j] = -1;
       if (knn_cnt) knn_cnt[qid] = 0;
     }
@@ -1132,7 +1142,7 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
   // the list holds point ids; the neighbours are gathered from their tree
   // positions (the index map's loads are independent and overlap)
   int n = 0;
-  if (knn_idx) {
+  if constexpr (ExcludesSelf<L>::value) {
     int c = 0;
     bool placed = false;
 #pragma unroll
@@ -1146,16 +1156,18 @@ k_normals(TreeView<T, 3> tv, L ld, const int* order, int order_mode, int m,
             lane_log[(n++) * 32] = own;
             placed = true;
           }
-          if (n < k) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
+          if (n < k) lane_log[(n++) * 32] = tv.pos_of(tv.fwd, top.id(j));
         }
       }
     }
     if (!placed && n < k) lane_log[(n++) * 32] = own;
     if (knn_cnt) knn_cnt[qid] = c;
   } else {
+    (void)knn_idx;
+    (void)knn_cnt;
 #pragma unroll
     for (int j = KMAX - 1; j >= 0; j--)
-      if (j < k && top.valid(j)) lane_log[(n++) * 32] = tv.fwd[top.id(j)];
+      if (j < k && top.valid(j)) lane_log[(n++) * 32] = tv.pos_of(tv.fwd, top.id(j));
   }
   if (PREC == PREC_FP64) {
     Sym3<double> C = log_covariance<T, double, DistT>(tv, lane_log, n, q);
@@ -1261,7 +1273,7 @@ __global__ void __launch_bounds__(QTHREADS) k_normals_rnear_warp(TreeView<T, 3> 
     for (int base = begin; base < begin + cnt; base += 32) {
       const int p = base + lane;
       if (p >= begin + cnt) continue;
-      const PointRec<T, 3> pr = tv.pts[p];
+      const PointRec<T, 3> pr = tv.pt(p);
       if (!whole && !(point_dist2<T, DistT, 3>(pr.c, q) < r2)) continue;
       const double e0 = (double)pr.c[0] - (double)q[0], e1 = (double)pr.c[1] - (double)q[1],
                    e2 = (double)pr.c[2] - (double)q[2];
@@ -1440,7 +1452,7 @@ __global__ void k_normals_pos(TreeView<T, 3> tv, L ld, const int* order, int ord
   const int32_t* P = pos + (int64_t)i * k;
   double s0 = 0, s1 = 0, s2 = 0;
   for (int j = 0; j < n; j++) {
-    const PointRec<T, 3> rp = tv.pts[P[j]];
+    const PointRec<T, 3> rp = tv.pt(P[j]);
     s0 += (double)rp.c[0] - (double)q[0];
     s1 += (double)rp.c[1] - (double)q[1];
     s2 += (double)rp.c[2] - (double)q[2];
@@ -1448,7 +1460,7 @@ __global__ void k_normals_pos(TreeView<T, 3> tv, L ld, const int* order, int ord
   const double inv = 1.0 / (double)n, a0 = s0 * inv, a1 = s1 * inv, a2 = s2 * inv;
   Sym3<double> C{0, 0, 0, 0, 0, 0};
   for (int j = 0; j < n; j++) {
-    const PointRec<T, 3> rp = tv.pts[P[j]];
+    const PointRec<T, 3> rp = tv.pt(P[j]);
     const double x = (double)rp.c[0] - (double)q[0] - a0, y = (double)rp.c[1] - (double)q[1] - a1,
                  z = (double)rp.c[2] - (double)q[2] - a2;
     C.a00 += x * x;

@@ -63,6 +63,25 @@ struct TreeView {
   int32_t root;     // TNode where this tree's traversals start
   const int32_t* fwd;  // original row -> tree position
   int32_t n_in;        // original rows (entries of fwd)
+  int32_t pts_cap;     // point records allocated (nv, or n for a capture-ready forest)
+  int* err;            // PPTKG_BOUNDS_CHECK builds: first failed check (site code); else null
+
+  // Index checks of the PPTKG_BOUNDS_CHECK build: an index outside [0, n)
+  // records `site` in *err (the first failure wins) and reads element 0
+  // instead, so a corrupt index is reported, never dereferenced.  In the
+  // normal build they are the identity.
+  __device__ __forceinline__ int checked(int i, int n, int site) const {
+#ifdef PPTKG_BOUNDS_CHECK
+    if (i < 0 || i >= n) {
+      if (err) atomicCAS(err, 0, site);
+      return 0;
+    }
+#endif
+    return i;
+  }
+  __device__ __forceinline__ const PointRec<T, D>& pt(int i) const { return pts[checked(i, pts_cap, 1)]; }
+  __device__ __forceinline__ int pos_of(const int32_t* map, int o) const { return map[checked(o, n_in, 2)]; }
+  __device__ __forceinline__ int node_index(int i) const { return checked(i, n_nodes, 3); }
 };
 
 // Host-side owner of one device tree, or of a forest of independent trees

@@ -113,6 +113,31 @@ def test_normals_match_fp64_oracle(gpu, port, dtype):
     assert np.percentile(ang, 99) <= 1e-4
 
 
+@pytest.mark.parametrize("dtype,precision", [(np.float64, "auto"), (np.float32, "fp64"), (np.float32, "auto")])
+def test_eigenvalues_relative_to_each_eigenvalue(gpu, port, dtype, precision):
+    # eigenvalues against the FP64 oracle, each to 1e-5 of itself (a floor
+    # of 1e-12 of the largest for eigenvalues at zero).  The FP32 path
+    # (float32 input, precision "auto") meets that for the two larger
+    # eigenvalues; its smallest keeps the absolute bound of 1e-5 of the
+    # largest: an FP32 eigensolve resolves an eigenvalue only to a few
+    # float32 ulps of the largest, which is more than 1e-5 of the smallest
+    # once the two differ by more than ~1e2 (a planar neighbourhood)
+    P = np.random.default_rng(2).random((100_000, 3)).astype(dtype)
+    ev, ew, sz = gpu.estimate_normals(P, 16, np.inf, output_eigenvalues=True, output_all_eigenvectors=True,
+                                      output_neighborhood_sizes=True, verbose=False, precision=precision)
+    _, _, osz, nb = port.port_estimate_normals(P, 16, np.inf, num_eigen=3, want_nbrs=True)
+    assert np.array_equal(sz, osz)
+    w, _, _ = port.normals_fp64(P, nb)
+    lmax = np.abs(w[:, 2:3])
+    err = np.abs(ew.astype(np.float64) - w)
+    rel_ok = err <= EVAL_TOL * np.abs(w) + 1e-12 * lmax
+    if dtype == np.float32 and precision == "auto":
+        assert rel_ok[:, 1:].all(), np.max(err[:, 1:] / np.abs(w[:, 1:]))
+        assert (err[:, 0] <= EVAL_TOL * lmax[:, 0]).all()
+    else:
+        assert rel_ok.all(), np.max(err / (np.abs(w) + 1e-300))
+
+
 def test_normals_with_radius_and_rnear_neighbourhoods(gpu, port):
     P = np.random.default_rng(1).random((40_000, 3)).astype(np.float32)
     out = gpu.estimate_normals(P, 20, 0.05, output_eigenvalues=True, output_all_eigenvectors=True,
