@@ -49,7 +49,7 @@ With one GPU the default run also measures the other configurations
 briefly (``configs``: the scene's kNN k=32 and r-near r=0.5 m, the 4,096-
 cloud ragged batch, the 64-tree serving mix) with 3 warm-up and at most 5
 timed steps each.  Bulky per-stage data is printed on ``{"detail": ...}``
-lines before the final JSON line, which keeps the figures that are judged.
+lines before the final JSON line, which keeps the headline figures.
 """
 import argparse
 import ctypes
@@ -1063,7 +1063,7 @@ def precision_report():
 WORKLOADS = {"serving": run_serving_workload, "plain": run_plain_workload, "ragged": run_ragged_workload,
              "multitree": run_multitree_workload, "scene": run_scene_workload}
 
-# keys of a workload's result that go to the detail lines (bulky, not judged)
+# keys of a workload's result that go to the detail lines (bulky, not headline figures)
 DETAIL_KEYS = ("stages_ms", "autotune", "precision", "rnear", "build", "graph_replay", "steps_note")
 
 
@@ -1084,7 +1084,7 @@ def _precision_summary(prec):
 
 
 def compact_serving(res):
-    """The main figures of the serving workload, in a few hundred bytes."""
+    """The headline figures of the serving workload, in a few hundred bytes."""
     plain = res.get("plain") or {}
     out = {"plain": {"value": plain.get("value"), "unit": "queries/s",
                      "p50_ms": (plain.get("latency") or {}).get("p50_ms"),
@@ -1135,7 +1135,7 @@ def run_config(name, args, ctx):
 
 
 def _round(x, digits=4):
-    """Floats to `digits` significant digits, recursively (keeps the judged
+    """Floats to `digits` significant digits, recursively (keeps the headline
     line short)."""
     if isinstance(x, float):
         return float(f"{x:.{digits}g}")
