@@ -598,10 +598,13 @@ struct Entry {
 };
 
 constexpr int SUB_THREADS = 256;
+// k_subtree nodes of at most this many points are split by one thread
+constexpr int LANE_NODE = 64;
 
-// Finishes small segments' whole subtrees in shared memory, one warp per
-// node, level by level.  Persistent: each CTA takes segments from the small
-// list until it is exhausted.  (Splitting the first levels' few nodes with
+// Finishes small segments' whole subtrees in shared memory, level by level:
+// one warp per node above LANE_NODE points, one thread per smaller node.
+// Persistent: each CTA takes segments from the small list until it is
+// exhausted.  (Splitting the first levels' few nodes with
 // the whole block instead was measured slower: a third more subtree time on
 // a 4,096-cloud forest; the warps of the SM's other CTAs already fill the
 // issue slots those levels leave idle.)
@@ -676,6 +679,7 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
       for (int ei = wid; ei < nA; ei += nw) {
         Entry<T, D> en = LA[ei];
         const int b = en.b, e = en.e, size = e - b;
+        if (size <= LANE_NODE) continue;  // (warp-uniform) one thread's node, below
         T mn[D], mx[D];
         for (int d = 0; d < D; d++) {
           mn[d] = Limits<T>::max();
@@ -801,6 +805,96 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
             else
               atomicExch(&cnt[3], 1);
           }
+        }
+      }
+      // nodes of at most LANE_NODE points: one thread each, with the
+      // reference's two converging cursors over shared memory (the pairs a
+      // warp forms by ranks), so that the many small nodes of the last
+      // levels do not each pay a warp's fixed per-node work
+      for (int ei = threadIdx.x; ei < nA; ei += blockDim.x) {
+        Entry<T, D> en = LA[ei];
+        const int b = en.b, e = en.e, size = e - b;
+        if (size > LANE_NODE) continue;
+        T mn[D], mx[D];
+        for (int d = 0; d < D; d++) {
+          mn[d] = Limits<T>::max();
+          mx[d] = Limits<T>::lowest();
+        }
+        for (int q = b; q < e; q++)
+          for (int d = 0; d < D; d++) {
+            const T x = X[d][q];
+            mn[d] = min(mn[d], x);
+            mx[d] = max(mx[d], x);
+          }
+        const int id = base + ei;
+        Rec<T, D> rec;
+        int act = 0, sd = 0;
+        T sv = (T)0;
+        node_logic<T, D>(size, seg.n_orig, en.parent < 0, en.lo, en.hi, mn, mx, max_leaf, thr, rec, act, sd, sv);
+        rec.begin = seg.b + b;
+        rec.end = seg.b + e;
+        if (id >= rec_cap) {
+          atomicExch(&ctl->status, 6);
+          continue;
+        }
+        recs[id] = rec;
+        if (en.parent >= 0) {
+          if (en.side == 0)
+            recs[en.parent].left = id;
+          else
+            recs[en.parent].right = id;
+        } else {
+          root_rec[-en.parent - 1] = id;
+        }
+        if (!act) continue;
+        const T* v = X[sd];
+        int L1 = 0, L2 = 0;
+        for (int q = b; q < e; q++) {
+          L1 += v[q] < sv;
+          L2 += v[q] <= sv;
+        }
+        for (int pass = 1; pass <= 2; pass++) {
+          const int Z = pass == 1 ? b + L1 : b + L2;
+          int i = pass == 1 ? b : b + L1, j = e - 1;
+          while (true) {
+            while (i < Z && !(pass == 1 ? !(v[i] < sv) : (v[i] > sv))) i++;
+            while (j >= Z && !(pass == 1 ? (v[j] < sv) : (v[j] <= sv))) j--;
+            if (i >= Z || j < Z) break;
+            for (int d = 0; d < D; d++) {
+              const T t = X[d][i];
+              X[d][i] = X[d][j];
+              X[d][j] = t;
+            }
+            const int t = ID[i];
+            ID[i] = ID[j];
+            ID[j] = t;
+            i++;
+            j--;
+          }
+        }
+        const int si = b + num_left_rule(L1, L2, size);
+        recs[id].split_index = seg.b + si;
+        for (int side = 0; side < 2; side++) {
+          const int cb = side ? si : b, ce = side ? e : si;
+          if (cb >= ce) continue;
+          Entry<T, D> c;
+          c.b = cb;
+          c.e = ce;
+          c.parent = id;
+          c.side = side;
+          for (int d = 0; d < D; d++) {
+            c.lo[d] = en.lo[d];
+            c.hi[d] = en.hi[d];
+          }
+          if (side == 0)
+            c.hi[sd] = sv;
+          else
+            c.lo[sd] = sv;
+          const int slot = atomicAdd(&cnt[1], 1);
+          if (slot < cap_list)
+            LB[slot] = c;
+          else
+            atomicExch(&cnt[3], 1);
         }
       }
       __syncthreads();
