@@ -599,7 +599,7 @@ struct Entry {
 
 constexpr int SUB_THREADS = 256;
 // k_subtree nodes of at most this many points are split by one thread
-constexpr int LANE_NODE = 64;
+constexpr int LANE_NODE = 32;
 
 // Finishes small segments' whole subtrees in shared memory, level by level:
 // one warp per node above LANE_NODE points, one thread per smaller node.
