@@ -436,7 +436,9 @@ __global__ void __launch_bounds__(BT) k_flags(int pass, Seg<T, D>* segs, const i
     int s, start, end;
     tile_at(segs, tile_seg, t, s, start, end);
     long long c = 0;
-    if (segs[s].act) {
+    // the second pass moves the points equal to the split value; with none
+    // (L1 == L2, the usual case for float data) it has nothing to do
+    if (segs[s].act && !(pass == 2 && segs[s].L1 == segs[s].L2)) {
       const T sv = segs[s].sv;
       const T* v = soa.x[segs[s].sd];
       const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2;
@@ -483,7 +485,7 @@ __global__ void __launch_bounds__(BT) k_scatter(int pass, Seg<T, D>* segs, const
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     int s, start, end;
     tile_at(segs, tile_seg, t, s, start, end);
-    if (!segs[s].act) continue;  // (uniform over the block)
+    if (!segs[s].act || (pass == 2 && segs[s].L1 == segs[s].L2)) continue;  // (uniform over the block)
     const T sv = segs[s].sv;
     const T* v = soa.x[segs[s].sd];
     const int b = segs[s].b, L1 = segs[s].L1, L2 = segs[s].L2, G = segs[s].G;
@@ -733,7 +735,7 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
           L2 += __popc(__ballot_sync(0xffffffffu, in && x <= sv));
         }
         const int half = size / 2;
-        for (int pass = 1; pass <= 2; pass++) {
+        for (int pass = 1; pass <= (L1 == L2 ? 1 : 2); pass++) {
           const int zlo = pass == 1 ? b : b + L1;
           const int Z = pass == 1 ? b + L1 : b + L2;
           int G = 0;
@@ -853,7 +855,7 @@ __global__ void __launch_bounds__(SUB_THREADS) k_subtree(const Seg<T, D>* small,
           L1 += v[q] < sv;
           L2 += v[q] <= sv;
         }
-        for (int pass = 1; pass <= 2; pass++) {
+        for (int pass = 1; pass <= (L1 == L2 ? 1 : 2); pass++) {
           const int Z = pass == 1 ? b + L1 : b + L2;
           int i = pass == 1 ? b : b + L1, j = e - 1;
           while (true) {
