@@ -23,6 +23,7 @@
 namespace pptkg {
 
 constexpr int BT = 256;     // threads per tile block
+constexpr int SWAP_U = 4;   // pairs a k_swap thread has in flight
 constexpr int TILE = 4096;  // points per tile
 constexpr int TITEMS = TILE / BT;
 
@@ -530,23 +531,49 @@ __global__ void __launch_bounds__(BT) k_swap(Seg<T, D>* segs, const int* tile_se
     tile_at(segs, tile_seg, t, s, start, end);
     if (!segs[s].act) continue;
     const int b = segs[s].b, e = segs[s].e, G = segs[s].G;
-    for (int i = start + threadIdx.x; i < end; i += BT) {
-      int j = i - b;
-      if (j >= G) break;
-      int x = blpos[b + j], y = grpos[b + j];
-      if (x < b || x >= e || y < b || y >= e) {
-        atomicExch(&ctl->status, 4);
-        continue;
+    // pair j of this tile: j = start - b + threadIdx.x + u * BT.  Every
+    // position belongs to one pair only, so the loads of SWAP_U pairs are
+    // issued before their stores: the swap is bound by memory latency, and
+    // one pair in flight per thread left most of it exposed
+    const int jend = min(end - b, G);
+    for (int j0 = start - b + threadIdx.x; j0 < jend; j0 += SWAP_U * BT) {
+      int x[SWAP_U], y[SWAP_U];
+      bool ok[SWAP_U];
+#pragma unroll
+      for (int u = 0; u < SWAP_U; u++) {
+        const int j = j0 + u * BT;
+        ok[u] = j < jend;
+        x[u] = ok[u] ? blpos[b + j] : b;
+        y[u] = ok[u] ? grpos[b + j] : b;
+        if (ok[u] && (x[u] < b || x[u] >= e || y[u] < b || y[u] >= e)) {
+          atomicExch(&ctl->status, 4);
+          ok[u] = false;
+        }
+      }
+      T vx[SWAP_U][D], vy[SWAP_U][D];
+      int ix[SWAP_U], iy[SWAP_U];
+#pragma unroll
+      for (int u = 0; u < SWAP_U; u++) {
+        if (!ok[u]) continue;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          vx[u][d] = soa.x[d][x[u]];
+          vy[u][d] = soa.x[d][y[u]];
+        }
+        ix[u] = soa.id[x[u]];
+        iy[u] = soa.id[y[u]];
       }
 #pragma unroll
-      for (int d = 0; d < D; d++) {
-        T tmp = soa.x[d][x];
-        soa.x[d][x] = soa.x[d][y];
-        soa.x[d][y] = tmp;
+      for (int u = 0; u < SWAP_U; u++) {
+        if (!ok[u]) continue;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          soa.x[d][x[u]] = vy[u][d];
+          soa.x[d][y[u]] = vx[u][d];
+        }
+        soa.id[x[u]] = iy[u];
+        soa.id[y[u]] = ix[u];
       }
-      int tmp = soa.id[x];
-      soa.id[x] = soa.id[y];
-      soa.id[y] = tmp;
     }
   }
 }
