@@ -163,11 +163,14 @@ class GpuEngine:
                 ev, = self._to_host([ev])
         return [ev[a:a + n] for a, n in spans]
 
-    def rnear(self, tree, queries, dmax, stream):
+    def rnear(self, tree, queries, dmax, stream, host=False):
         from . import kdtree
         with self.torch.cuda.stream(stream):
             q = self.torch.as_tensor(queries, device=self.device)
-            return kdtree.rnear(tree, q, dmax)
+            off, hits = kdtree.rnear(tree, q, dmax)
+            if host:
+                return off.cpu().numpy(), hits.cpu().numpy()
+            return off, hits
 
     def synchronize(self, stream):
         stream.synchronize()
@@ -333,11 +336,13 @@ class Server:
                       key=("normals", int(k), float(r), precision, host))
         return self._submit(req)
 
-    def rnear(self, tree_id, queries, dmax):
+    def rnear(self, tree_id, queries, dmax, to_host=None):
         """Future of (offsets m + 1, hits) of the points within dmax of each
-        query point, in the reference's order."""
+        query point, in the reference's order.  to_host as for knn (default:
+        numpy results when the queries are a numpy array)."""
         m = int(queries.shape[0])
-        return self._submit(Request("rnear", (tree_id, queries, float(dmax)), m * QUERY_BYTES * 8, m))
+        host = isinstance(queries, np.ndarray) if to_host is None else bool(to_host)
+        return self._submit(Request("rnear", (tree_id, queries, float(dmax), host), m * QUERY_BYTES * 8, m))
 
     def drop(self, tree_id):
         """Releases a resident tree."""
@@ -493,6 +498,10 @@ class Server:
                     kl = max(s.r.args[2] for s in ss)
                     res = self.engine.knn_batch(trees, [_rows(s.r.args[1], s.lo, s.hi) for s in ss], kl, key[2],
                                                 stream, host=key[4])
+                    # (host results arrive by asynchronous copies: the counts are
+                    # capped only once the stream has finished them)
+                    if key[4]:
+                        self.engine.synchronize(stream)
                     res = [_first_k(i, c, s.r.args[2], kl) for (i, c), s in zip(res, ss)]
                     self._finish(ss, res, stream)
                 elif kind == "normals":
@@ -502,7 +511,7 @@ class Server:
                     self._finish(ss, res, stream)
                 elif kind == "rnear":
                     r = ss[0].r
-                    res = self.engine.rnear(self.trees[r.args[0]], r.args[1], r.args[2], stream)
+                    res = self.engine.rnear(self.trees[r.args[0]], r.args[1], r.args[2], stream, host=r.args[3])
                     self._finish(ss, [res], stream)
             if marks:
                 e1 = self.engine.mark(stream)

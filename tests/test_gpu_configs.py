@@ -12,6 +12,10 @@
 * 4,096 ragged clouds (158M points): one forest build, kNN k=16 and normals
   for every point; sampled clouds exact against the oracle, properties on
   every row.
+* The 64-tree serving mix at a tenth of its point count (64 lidar scenes of
+  50k-400k points): a burst of kNN (k 8..64), r-near (r 0.1..1 m), normal
+  and build requests through the server, every answer equal to the direct
+  single-tree call on the same tree.
 
 The oracle runs on the host over the same seeded inputs; neighbourhoods for
 the FP64 normal oracle come from the oracle's own kNN (ties by point index).
@@ -161,3 +165,58 @@ def test_rnear_normals_match_fp64_oracle(gpu, port):
     dots = np.abs((ev[keep, 0, :].astype(np.float64) * V[:, :, 0]).sum(1))
     assert (dots[ok] >= 1 - DOT_TOL).all(), np.sort(dots[ok])[:5]
     assert ok.sum() > 0.95 * keep.sum()
+
+
+def test_multitree_mix_shape(gpu):
+    import threading
+    from pptk_b200 import estimate_normals, kdtree, serving, synth
+    rng = np.random.default_rng(17)
+    sizes = rng.integers(50_000, 400_001, 64)
+    clouds = [synth.lidar_scene(int(n), seed=300 + i) for i, n in enumerate(sizes)]
+    srv = serving.Server(budget_bytes=40e9, slots=3)
+    ids = [f.result(timeout=300) for f in [srv.build(c) for c in clouds]]
+    reqs = []
+    for _ in range(240):
+        u = rng.random()
+        g = int(rng.integers(0, 64))
+        m = int(np.exp(rng.uniform(np.log(1e3), np.log(5e4))))
+        if u < 0.05:
+            reqs.append(("build", g, synth.lidar_scene(int(rng.integers(20_000, 200_000)), seed=int(rng.integers(1e6)))))
+        elif u < 0.45:
+            q = clouds[g][rng.integers(0, len(clouds[g]), m)] + np.float32(5e-3)
+            reqs.append(("knn", g, (q, int(rng.integers(8, 65)))))
+        elif u < 0.60:
+            q = clouds[g][rng.integers(0, len(clouds[g]), min(m, 2_000))]
+            reqs.append(("rnear", g, (q, float(np.float32(rng.uniform(0.1, 1.0))))))
+        else:
+            reqs.append(("normals", g, rng.integers(0, len(clouds[g]), m).astype(np.int32)))
+
+    def submit(kind, g, a):
+        if kind == "knn":
+            return srv.knn(ids[g], a[0], k=a[1])
+        if kind == "rnear":
+            return srv.rnear(ids[g], a[0], a[1])
+        if kind == "normals":
+            return srv.normals(ids[g], a, k=16)
+        return srv.build(a)
+
+    futs = [submit(*r) for r in reqs]
+    results = [f.result(timeout=600) for f in futs]
+    for (kind, g, a), got in zip(reqs, results):
+        tree = srv.trees[ids[g]]
+        if kind == "knn":
+            direct, cnt = kdtree.knn(tree, a[0], a[1])
+            assert np.array_equal(got[0], direct) and np.array_equal(got[1], cnt), (g, a[1])
+        elif kind == "rnear":
+            off, hits = kdtree.rnear(tree, a[0], a[1])
+            assert np.array_equal(got[0], off) and np.array_equal(got[1], hits), g
+        elif kind == "normals":
+            direct = estimate_normals(clouds[g], 16, np.inf, subsample=a, verbose=False)
+            assert np.array_equal(np.nan_to_num(got, nan=-9.0), np.nan_to_num(direct, nan=-9.0)), g
+        else:
+            q = a[:300] + np.float32(1e-3)
+            direct, _ = kdtree.knn(kdtree._build(a), q, 8)
+            assert np.array_equal(srv.knn(got, q, k=8).result(timeout=120)[0], direct)
+    st = srv.stats()
+    assert st["knn"]["requests"] + st["rnear"]["requests"] + st["normals"]["requests"] >= 200
+    srv.close()

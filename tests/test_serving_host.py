@@ -47,7 +47,7 @@ class FakeEngine:
             self.batches.append(("normals", len(trees)))
         return [np.zeros((t.n if i is None else len(i), 3)) for t, i in zip(trees, indices)]
 
-    def rnear(self, tree, queries, dmax, stream):
+    def rnear(self, tree, queries, dmax, stream, host=False):
         return ([0], [])
 
     def synchronize(self, stream):
@@ -290,4 +290,51 @@ def test_deferral_ends_after_defer_ms():
     assert time.perf_counter() - t0 >= 0.04
     assert not blocker.done()
     late.result(timeout=10)
+    srv.close()
+
+
+class AsyncHostEngine(FakeEngine):
+    """Host results that, like pinned copies on a stream, are only filled in
+    when the stream is synchronised."""
+
+    def __init__(self):
+        super().__init__()
+        self.pending = []
+
+    def knn_batch(self, trees, queries, k, dmax, stream, host=False):
+        out = super().knn_batch(trees, queries, k, dmax, stream, host)
+        empty = []
+        for idx, cnt in out:
+            e_idx, e_cnt = np.zeros_like(idx), np.zeros_like(cnt)
+            self.pending.append((e_idx, idx, e_cnt, cnt))
+            empty.append((e_idx, e_cnt))
+        return empty
+
+    def synchronize(self, stream):
+        with self.lock:
+            for e_idx, idx, e_cnt, cnt in self.pending:
+                e_idx[...] = idx
+                e_cnt[...] = cnt
+            self.pending = []
+
+
+def test_knn_counts_of_a_merged_launch_wait_for_the_host_copies():
+    # requests of one k class run at the class's largest k; each takes its
+    # first k columns and its count capped at k -- only after the host
+    # copies have landed
+    eng = AsyncHostEngine()
+    srv = serving.Server(budget_bytes=1e9, slots=1, engine=eng)
+    rng = np.random.default_rng(8)
+    pts = rng.random((300, 3))
+    tid = srv.build(pts).result(timeout=10)
+    blocker = srv.knn(tid, rng.random((3, 3)), k=8)
+    wait_started(eng, "knn")
+    qs = [rng.random((10, 3)) for _ in range(2)]
+    futs = [srv.knn(tid, qs[0], k=5), srv.knn(tid, qs[1], k=7)]
+    blocker.result(timeout=10)
+    for q, f, k in zip(qs, futs, (5, 7)):
+        idx, cnt = f.result(timeout=10)
+        d = ((q[:, None, :] - pts[None]) ** 2).sum(-1)
+        assert np.array_equal(idx, np.argsort(d, axis=1, kind="stable")[:, :k])
+        assert (cnt == k).all()
     srv.close()
