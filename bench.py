@@ -1064,7 +1064,7 @@ WORKLOADS = {"serving": run_serving_workload, "plain": run_plain_workload, "ragg
              "multitree": run_multitree_workload, "scene": run_scene_workload}
 
 # keys of a workload's result that go to the detail lines (bulky, not headline figures)
-DETAIL_KEYS = ("stages_ms", "autotune", "precision", "rnear", "build", "graph_replay", "steps_note")
+DETAIL_KEYS = ("stages_ms", "autotune", "precision", "rnear", "build", "steps_note")
 
 
 def _lat(d):
