@@ -85,7 +85,7 @@ def parse():
     p.add_argument("--max-batch", type=int, default=20_000_000, help="queries folded into one server batch")
     p.add_argument("--batch-ms", type=float, default=None,
                    help="time budget of one server batch (None: batches capped by --max-batch only)")
-    p.add_argument("--max-host-batch", type=int, default=8_000_000,
+    p.add_argument("--max-host-batch", type=int, default=20_000_000,
                    help="queries folded into one server batch that returns numpy results")
     p.add_argument("--plain-sample", type=int, default=24, help="requests timed through the plain calls")
     p.add_argument("--latency-seconds", type=float, default=3.0)
